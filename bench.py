@@ -1,0 +1,579 @@
+"""Benchmark of the benchNTT hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Headline workload (one "step"): the uneven batch -- 100,000 forward 128-bit
+NTTs with N log-uniform over 2^4..2^10 plus 64 at 2^16 and 4 at 2^20 (modulus
+2^124 - 719 of the reference NTT drivers), run by one graph launch of the
+persistent work-queue kernel.  `value` is transforms per second with inputs
+resident in HBM; `e2e` is the same metric through bntt_batch_run_host from
+pinned host buffers (copies in and out inside the timed region).  The same
+line carries the per-call GPU path on the same jobs, the BLAS ops at 2^24
+elements in GB/s, uniform batches of 65,536 transforms per size, the roofline
+of the persistent kernel against the measured IMAD pipe peak, the reference's
+CPU throughput on the same workload (timed on this host's cores), and the SM
+clocks sampled during the timed region.
+
+Under torchrun (N > 1) every rank runs the same per-GPU batch on its own GPU
+(no data exchange: the transforms are independent), the timed region is
+bracketed by barriers and the slowest rank's time is used.
+
+--impl reference times the reference's own CPU implementation (AVX-512 build
+when the host has it, else AVX2, else scalar; compiled from the benchNTT
+sources into oracle/_ref) on the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "batched 128b NTT/s and BLAS GB/s vs per-call GPU path; bit-exact; p99 latency"
+UNIT = "NTT/s"
+Q_NTT = (1152921504606846975 << 64) | 18446744073709550897
+MU_NTT = (9223372036854775808 << 64) | 5752
+Q_BLAS = (0x0FFFFFFFFFFFFFFF << 64) | 0xFFFFFFFFFFFFFFC5
+MU_BLAS = (0x8000000000000000 << 64) | 0x1D8
+AXPY_X = (208488538572646751 << 64) | 12808410693871070164
+IMAD_PER_BUTTERFLY = 80      # generic 32-bit-limb Barrett mulmod (algorithmic count)
+HBM_BYTES_PER_ELEM_BLAS = 48  # two 16-byte reads and one write
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="fraction of the uneven batch (profiling captures of a smaller case)")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="only the persistent-kernel step (for profiler launch lists)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------- distributed
+class Dist:
+    def __init__(self, want: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.25)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[4:]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        max_mhz = max(r[1] for r in rows)
+        peak_p = max(r[2] for r in rows)
+        loaded = [r for r in rows if r[2] >= 0.5 * peak_p] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in loaded for i, v in enumerate(r[3][1:5])
+                          if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max_mhz,
+                "reasons": reasons, "samples": len(rows), "samples_under_load": len(loaded),
+                "power_w_max": peak_p}
+
+
+# ---------------------------------------------------------------- CPU side
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def ref_impl() -> tuple[str, str]:
+    """(implementation, kind) of the CPU baseline available on this host."""
+    flags = ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("flags"):
+                flags = line
+                break
+    except OSError:
+        pass
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    for impl, need in (("avx512", ("avx512f", "avx512dq")), ("avx2", ("avx2",)), ("scalar", ())):
+        if all(f in flags.split() for f in need) and \
+                os.path.exists(os.path.join(ref_dir, f"libref_ntt_{impl}_10.so")):
+            return impl, "reference"
+    return "oracle", "port"
+
+
+class CpuNtt:
+    """The reference's per-size NTT functions (or the oracle restatement)."""
+
+    def __init__(self):
+        self.impl, self.kind = ref_impl()
+        self.libs = {}
+
+    def lib(self, logn: int):
+        if logn not in self.libs:
+            if self.kind == "reference":
+                l = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref",
+                                             f"libref_ntt_{self.impl}_{logn}.so"))
+                l.bntt_ref_ntt_batch.restype = ctypes.c_double
+                l.bntt_ref_ntt_batch.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_size_t] + \
+                    [ctypes.c_uint64] * 4 + [ctypes.c_int]
+            else:
+                path = os.path.join(ROOT, "oracle", "liboracle.so")
+                if not os.path.exists(path):
+                    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"],
+                                   check=True, stdout=subprocess.DEVNULL)
+                l = ctypes.CDLL(path)
+                l.orc_ntt_batch.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_size_t] + \
+                    [ctypes.c_uint64] * 4 + [ctypes.c_int, ctypes.c_int]
+            self.libs[logn] = l
+        return self.libs[logn]
+
+    def run(self, logn, y, x, t, count, threads) -> float:
+        """Seconds for `count` transforms of size 2^logn on `threads` threads."""
+        l = self.lib(logn)
+        args = (y.ctypes.data, x.ctypes.data, t.ctypes.data)
+        qm = (Q_NTT >> 64, Q_NTT & (2**64 - 1), MU_NTT >> 64, MU_NTT & (2**64 - 1))
+        if self.kind == "reference":
+            return l.bntt_ref_ntt_batch(*args, count, *qm, threads)
+        t0 = time.perf_counter()
+        l.orc_ntt_batch(y.ctypes.data, x.ctypes.data, t.ctypes.data, logn, count, *qm, 0, threads)
+        return time.perf_counter() - t0
+
+
+def cpu_uneven_throughput(batch, budget_s: float, threads: int, cpu: CpuNtt = None) -> dict:
+    """Reference throughput on the uneven batch from a bounded, stratified
+    sample: per size, a sample of transforms run on all threads gives the
+    per-transform CPU cost c_N (thread-seconds); the batch then needs
+    max(sum(count_N * c_N) / threads, max c_N) seconds with perfect packing."""
+    import benchntt_b200 as bn
+    cpu = cpu or CpuNtt()
+    counts = {int(n): int((batch.logns == n).sum()) for n in batch.sizes}
+    cost = {}
+    per_size = budget_s / len(counts)
+    for n, cnt in sorted(counts.items()):
+        size = 1 << n
+        t = bn.fill_uniform(2000 + n, size, Q_NTT)
+        k = min(cnt, max(1, threads))
+        k_max = max(k, min(cnt, int(2e8 // (16 * size))))
+        xs = bn.fill_uniform(11, size * k_max, Q_NTT)
+        y = np.empty_like(xs)
+        used = min(threads, k)
+        dt = cpu.run(n, y, xs, t, k, used)          # first pass sizes the sample
+        reps = k
+        while dt < per_size * 0.5 and reps < k_max:
+            reps = min(k_max, max(reps * 2, int(reps * per_size / max(dt, 1e-6) * 0.5)))
+            used = min(threads, reps)
+            dt = cpu.run(n, y[: reps * size], xs[: reps * size], t, reps, used)
+        cost[n] = dt * used / reps
+    work = sum(counts[n] * cost[n] for n in counts)
+    t_batch = max(work / threads, max(cost.values()))
+    return {"value": batch.count / t_batch, "unit": UNIT, "cores": threads, "kind": cpu.kind,
+            "impl": cpu.impl,
+            "sample": ("stratified: per size, a timed sample of transforms on all threads "
+                       "gives the per-transform CPU cost; batch time = max(sum(count*cost)/cores, "
+                       "max cost); sample budget %.0f s" % budget_s),
+            "seconds_per_transform": {str(1 << n): cost[n] for n in sorted(cost)},
+            "batch_seconds": t_batch}
+
+
+# ------------------------------------------------------------- GPU helpers
+def cuda_events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def profiles_traffic(name: str):
+    """traffic_bytes_per_launch recorded in profiles/<name>.md (ncu capture)."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(path):
+            if line.strip().startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1].split()[0])
+    except (OSError, ValueError):
+        return None
+    return None
+
+
+def run_ours(args, dist: Dist):
+    import torch
+
+    import benchntt_b200 as bn
+    from benchntt_b200 import workloads as W
+
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    ctx = bn.Context(dev, stream=stream.cuda_stream)
+    L = bn.lib()
+    out = {}
+
+    # ---------------------------------------------------- headline workload
+    batch = W.uneven_batch()
+    if args.scale < 1.0:
+        n_small = max(1, int(100_000 * args.scale))
+        large = tuple((l, max(1, int(c * args.scale))) for l, c in ((16, 64), (20, 4)))
+        batch = W.uneven_batch(n_small=n_small, large=large)
+    mod = bn.modulus(Q_NTT, MU_NTT)
+    plans = {n: bn.Plan(ctx, n, Q_NTT, MU_NTT,
+                        bn.fill_uniform(W.SEED_TWIDDLE_BASE + n, 1 << n, Q_NTT))
+             for n in batch.sizes}
+    pid = {n: i for i, n in enumerate(batch.sizes)}
+    x = torch.empty((batch.total, 2), dtype=torch.int64, device=dev)
+    y = torch.empty_like(x)
+    bn.check(L.bntt_fill_uniform_dev(ctx.handle, x.data_ptr(), batch.total, W.SEED_INPUT, 0,
+                                     ctypes.byref(mod), 0))
+    engine = bn.Batch(ctx, [plans[n] for n in batch.sizes])
+    offs = batch.offsets * 16
+    jobs = bn.Batch.jobs([x.data_ptr() + int(o) for o in offs], [y.data_ptr() + int(o) for o in offs],
+                         [pid[int(n)] for n in batch.logns])
+    for _ in range(args.warmup):
+        engine.run_dev(jobs)
+    ctx.synchronize()
+    if engine.status() != bn.OK:
+        raise RuntimeError("batch kernel reported a timed-out wait")
+    clocks = ClockSampler(dev)
+    clocks.start()
+    dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launches
+    e0, e1 = cuda_events()
+    e0.record(stream)
+    for _ in range(args.steps):
+        engine.run_dev(jobs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    gpu_launches = ctx.launches - launches0
+    ms_local = e0.elapsed_time(e1) / args.steps
+    ms = dist.max(ms_local)
+    value = batch.count * dist.world / (ms * 1e-3)
+
+    # roofline of the persistent kernel (one launch per step)
+    bfly = batch.butterflies
+    imad_peak = ctx.imad_peak()
+    achieved = IMAD_PER_BUTTERFLY * bfly / (ms_local * 1e-3)
+    alg_bytes = 32.0 * batch.total      # read every input, write every output once
+    traffic = profiles_traffic("k_batch_uneven.md")
+    if traffic is not None and args.scale < 1.0:
+        traffic = None
+    peaks = measured_peaks()
+    roofline = {
+        "bound": "imad", "kernel": "k_batch (persistent work queue)",
+        "achieved": achieved / 1e12, "peak": imad_peak / 1e12, "unit": "T IMAD-op/s",
+        "frac": achieved / imad_peak, "peak_source": "measured live: bntt_probe_imad_peak",
+        "algorithmic": f"{IMAD_PER_BUTTERFLY} IMAD per butterfly x {bfly} butterflies per launch",
+        "traffic": traffic,
+        "hbm": {"achieved_gbs": alg_bytes / (ms_local * 1e-3) / 1e9,
+                "peak_gbs": peaks.get("hbm_gbs"), "algorithmic_bytes": alg_bytes,
+                "frac": (alg_bytes / (ms_local * 1e-3) / 1e9) / peaks["hbm_gbs"]
+                if peaks.get("hbm_gbs") else None,
+                "peak_source": "MEASURED_PEAKS.json" if peaks.get("from_file") else "fallback"},
+    }
+
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u128 (4 x u32 limbs, exact integer)",
+        "data": "synthetic: seeded uniform residues in [0, q) and seeded per-size twiddle tables",
+        "config": {"workload": "uneven_batch", "transforms": batch.count,
+                   "sizes": "100,000 x N=2^4..2^10 (log-uniform) + 64 x 2^16 + 4 x 2^20"
+                   if args.scale == 1.0 else f"scaled x{args.scale}",
+                   "modulus": "2^124-719 (src/ntt_scalar.c:633)",
+                   "l2": f"inputs {batch.total * 16 / 1e6:.0f} MB > 126 MB L2 (no flush needed)",
+                   "parallelism": f"independent batch per GPU x{dist.world}",
+                   "launch": "one CUDA-graph launch of the persistent kernel per step"},
+        "gpu_launches": gpu_launches,
+        "roofline": roofline,
+        "clocks": clk,
+        "parity": "bit-exact vs the reference: tests/test_gpu_batch.py::test_full_uneven_batch_matches_oracle",
+    }
+    if args.headline_only:
+        return result, ctx
+
+    # ------------------------------------------------------------ e2e (host)
+    result["e2e"] = e2e_uneven(args, dist, ctx, engine, batch, pid)
+    # ---------------------------------------------------------- per-call path
+    result["per_call"] = per_call(args, dist, ctx, stream, engine, jobs, batch, value)
+    # ----------------------------------------------------------------- BLAS
+    result["blas"] = blas_bench(args, ctx, stream, peaks)
+    # --------------------------------------------------------- uniform sizes
+    result["uniform"] = uniform_bench(args, ctx, stream, imad_peak)
+    engine.close()
+    del x, y
+    for p in plans.values():
+        p.close()
+    return result, ctx
+
+
+def measured_peaks() -> dict:
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        d["from_file"] = True
+        return d
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "from_file": False}
+
+
+def e2e_uneven(args, dist, ctx, engine, batch, pid) -> dict:
+    """bntt_batch_run_host from pinned host buffers: every step copies all
+    inputs in and all outputs out."""
+    import torch
+
+    import benchntt_b200 as bn
+    xh = torch.empty((batch.total, 2), dtype=torch.int64, pin_memory=True)
+    yh = torch.empty_like(xh, pin_memory=True)
+    L = bn.lib()
+    mod = bn.modulus(Q_NTT, MU_NTT)
+    bn.check(L.bntt_fill_uniform_host(xh.data_ptr(), batch.total, 11, 0, ctypes.byref(mod), 0))
+    offs = batch.offsets * 16
+    hjobs = bn.Batch.jobs([xh.data_ptr() + int(o) for o in offs],
+                          [yh.data_ptr() + int(o) for o in offs], [pid[int(n)] for n in batch.logns])
+    steps = max(3, min(args.steps, 10))
+    for _ in range(max(1, min(args.warmup, 3))):
+        engine.run_host(hjobs)
+    dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        engine.run_host(hjobs)
+    dt = (time.perf_counter() - t0) / steps
+    dt = dist.max(dt)
+    nbytes = batch.total * 16
+    del xh, yh
+    return {"value": batch.count * dist.world / dt, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+            "d2h_bytes_per_step": nbytes, "ms_per_step": dt * 1e3, "steps": steps,
+            "api": "bntt_batch_run_host (pinned host buffers; pipelined copies)",
+            "pcie_gbs_each_way": nbytes / dt / 1e9}
+
+
+def per_call(args, dist, ctx, stream, engine, jobs, batch, batched_value) -> dict:
+    """The same jobs, one launch per transform (per HBM pass above 2^10)."""
+    import torch
+    engine.run_percall_dev(jobs)   # warm-up pass
+    ctx.synchronize()
+    launches = 0
+    e0, e1 = cuda_events()
+    reps = 2
+    e0.record(stream)
+    for _ in range(reps):
+        engine.run_percall_dev(jobs)
+        launches += engine.last_launches
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = dist.max(e0.elapsed_time(e1) / reps)
+    v = batch.count * dist.world / (ms * 1e-3)
+    return {"value": v, "unit": UNIT, "ms_per_step": ms, "launches_per_step": launches // reps,
+            "batched_over_per_call": batched_value / v}
+
+
+def blas_bench(args, ctx, stream, peaks) -> dict:
+    import torch
+
+    import benchntt_b200 as bn
+    L = bn.lib()
+    n = 1 << 24
+    mod = bn.modulus(Q_BLAS, MU_BLAS)
+    a = torch.empty((n, 2), dtype=torch.int64, device=ctx.device)
+    b = torch.empty_like(a)
+    c = torch.empty_like(a)
+    bn.check(L.bntt_fill_uniform_dev(ctx.handle, a.data_ptr(), n, 3000, 0, ctypes.byref(mod), 0))
+    bn.check(L.bntt_fill_uniform_dev(ctx.handle, b.data_ptr(), n, 4000, 0, ctypes.byref(mod), 0))
+    res = {"length": n, "bytes_per_op": HBM_BYTES_PER_ELEM_BLAS * n,
+           "peak_gbs": peaks.get("hbm_gbs"),
+           "peak_source": "MEASURED_PEAKS.json" if peaks.get("from_file") else "fallback",
+           "note": "operands 256 MiB each > L2: no flush needed"}
+    for op in ("vvadd", "vvsub", "vvmul", "axpy"):
+        fn = getattr(L, f"bntt_{op}_dev")
+
+        def go():
+            if op == "axpy":
+                bn.check(fn(ctx.handle, c.data_ptr(), a.data_ptr(), b.data_ptr(), bn.U128.of(AXPY_X),
+                            n, ctypes.byref(mod), 0))
+            else:
+                bn.check(fn(ctx.handle, c.data_ptr(), a.data_ptr(), b.data_ptr(), n,
+                            ctypes.byref(mod), 0))
+        for _ in range(max(3, args.warmup)):
+            go()
+        e0, e1 = cuda_events()
+        reps = max(5, args.steps)
+        e0.record(stream)
+        for _ in range(reps):
+            go()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gbs = HBM_BYTES_PER_ELEM_BLAS * n / (ms * 1e-3) / 1e9
+        res[op] = {"gbs": gbs, "ms": ms, "frac_of_hbm_peak": gbs / peaks["hbm_gbs"]}
+    del a, b, c
+    return res
+
+
+def uniform_bench(args, ctx, stream, imad_peak) -> dict:
+    """65,536 transforms of one size, one launch (config: uniform batch)."""
+    import torch
+
+    import benchntt_b200 as bn
+    L = bn.lib()
+    mod = bn.modulus(Q_NTT, MU_NTT)
+    res = {}
+    count = 65536
+    for logn in range(4, 11):
+        n = 1 << logn
+        x = torch.empty((n * count, 2), dtype=torch.int64, device=ctx.device)
+        y = torch.empty_like(x)
+        bn.check(L.bntt_fill_uniform_dev(ctx.handle, x.data_ptr(), n * count, 7, 0,
+                                         ctypes.byref(mod), 0))
+        plan = bn.Plan(ctx, logn, Q_NTT, MU_NTT, bn.fill_uniform(2000 + logn, n, Q_NTT))
+        for _ in range(3):
+            plan.forward(y, x, count)
+        e0, e1 = cuda_events()
+        reps = max(5, args.steps // 2)
+        e0.record(stream)
+        for _ in range(reps):
+            plan.forward(y, x, count)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        bfly = count * (n // 2) * logn
+        res[str(n)] = {"ntt_per_s": count / (ms * 1e-3), "ms": ms,
+                       "imad80_frac": IMAD_PER_BUTTERFLY * bfly / (ms * 1e-3) / imad_peak}
+        plan.close()
+        del x, y
+    return res
+
+
+# ---------------------------------------------------------- reference arm
+def run_reference(args, dist: Dist):
+    from benchntt_b200 import workloads as W
+    if dist.rank != 0:
+        return None
+    batch = W.uneven_batch()
+    threads = cpu_threads()
+    cpu = CpuNtt()
+    budget = max(1.0, min(6.0, 150.0 / max(1, args.steps + args.warmup)))
+    vals = []
+    last = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_uneven_throughput(batch, budget, threads, cpu)
+        if i >= args.warmup:
+            vals.append(r["value"])
+            last = r
+    value = statistics.median(vals)
+    last["value"] = value
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * batch.count / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u128 (uint128_t / 2 x u64)",
+        "data": "synthetic: seeded uniform residues in [0, q), seeded per-size twiddle tables",
+        "config": {"workload": "uneven_batch", "transforms": batch.count,
+                   "sizes": "100,000 x N=2^4..2^10 (log-uniform) + 64 x 2^16 + 4 x 2^20",
+                   "modulus": "2^124-719 (src/ntt_scalar.c:633)",
+                   "parallelism": f"{threads} host threads"},
+        "cpu_baseline": last,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    dist = Dist(args.gpus)
+    try:
+        if args.impl == "reference":
+            res = run_reference(args, dist)
+            if res is not None:
+                print(json.dumps(res), flush=True)
+            return
+        res, ctx = run_ours(args, dist)
+        if dist.rank == 0 and dist.world == 1 and not args.no_cpu and not args.headline_only:
+            from benchntt_b200 import workloads as W
+            res["cpu_baseline"] = cpu_uneven_throughput(W.uneven_batch(), 12.0, cpu_threads())
+            res["gpu_over_cpu"] = res["value"] / res["cpu_baseline"]["value"]
+            res["e2e_over_cpu"] = res["e2e"]["value"] / res["cpu_baseline"]["value"]
+        if dist.rank == 0:
+            print(json.dumps(res), flush=True)
+        ctx.close()
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,451 @@
+// batch.cu -- host side of the batch engine (schedules, uploads, CUDA graphs)
+// and the bntt_batch_* entry points.  Device code: batch_dev.cuh,
+// instantiated in batch_kfast.cu / batch_kref.cu.
+#include <algorithm>
+#include <cstring>
+
+#include "batch_dev.cuh"
+
+namespace bntt {
+
+const void* batch_kernel_fast();
+const void* batch_kernel_ref();
+
+static size_t shape_smem(int s) {
+  const BatchShape& b = kShapes[s];
+  const int npass = (b.m + b.logr - 1) / b.logr;
+  return npass > 1 ? (size_t)b.tpc * ((size_t)1 << b.m) * 16 : 0;
+}
+
+// First shape for (m, map) with the preferred radix (0 = any).
+int batch_shape_for(int m, int map, int logr_pref) {
+  for (int s = 0; s < kNumShapes; ++s)
+    if (kShapes[s].m == m && kShapes[s].map == map && (logr_pref ? kShapes[s].logr == logr_pref : true))
+      return s;
+  return -1;
+}
+
+// Shape choice per size: small tiles, interleaved passes, contiguous passes.
+struct ShapeChoice {
+  int small[11];
+  int pass_il[11];
+  int pass_contig[11];
+};
+
+// One job list turned into work items, with its device copies and graph.
+struct Schedule {
+  std::vector<DevJob> djobs;
+  std::vector<uint32_t> order;
+  std::vector<WorkItem> items;
+  std::vector<uint32_t> pass_tiles;
+  size_t nslots = 0;
+  void* d_jobs = nullptr;
+  size_t d_jobs_cap = 0;
+  void* d_order = nullptr;
+  size_t d_order_cap = 0;
+  void* d_items = nullptr;
+  size_t d_items_cap = 0;
+  void* d_ctl = nullptr;
+  size_t d_ctl_cap = 0;
+  void* d_pass_tiles = nullptr;
+  size_t d_pass_tiles_cap = 0;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t exec_stream = nullptr;  // stream the graph was captured on
+  int grid = 0;
+  size_t smem = 0;
+};
+
+}  // namespace bntt
+
+using namespace bntt;
+
+struct bntt_batch {
+  bntt_ctx* ctx = nullptr;
+  std::vector<bntt_plan*> plans;
+  ModParams mp{};
+  bool fast = false;
+  int layout = 0;
+  ShapeChoice shapes{};
+  // device-pointer runs
+  std::vector<bntt_job> last_jobs;
+  Schedule main;
+  // host-pointer runs: packed device region, job groups with own schedules
+  std::vector<bntt_job> host_last_jobs;
+  std::vector<Schedule> groups;
+  std::vector<size_t> group_first;   // first job of each group (+ end)
+  std::vector<size_t> dev_off;       // byte offset of each job in the region
+  void* region = nullptr;
+  size_t region_cap = 0;
+  size_t last_launches = 0;
+};
+
+namespace bntt {
+
+static int grow(bntt_ctx* c, void** p, size_t* cap, size_t bytes) {
+  if (*cap >= bytes && *p) return BNTT_OK;
+  if (*p) ctx_free(c, *p);
+  *p = nullptr;
+  *cap = 0;
+  const size_t want = std::max<size_t>(bytes, 256);
+  if (int rc = ctx_alloc(c, p, want)) return rc;
+  *cap = want;
+  return BNTT_OK;
+}
+
+static void free_schedule(bntt_ctx* c, Schedule& s) {
+  if (s.exec) cudaGraphExecDestroy(s.exec);
+  s.exec = nullptr;
+  for (void** p : {&s.d_jobs, &s.d_order, &s.d_items, &s.d_ctl, &s.d_pass_tiles}) {
+    if (*p) ctx_free(c, *p);
+    *p = nullptr;
+  }
+  s.d_jobs_cap = s.d_order_cap = s.d_items_cap = s.d_ctl_cap = s.d_pass_tiles_cap = 0;
+}
+
+static const void* batch_kernel(bool fast) { return fast ? batch_kernel_fast() : batch_kernel_ref(); }
+
+static int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count) {
+  sc.djobs.resize(count);
+  sc.order.clear();
+  sc.items.clear();
+  sc.pass_tiles.clear();
+  sc.nslots = 0;
+  std::vector<uint32_t> by_size[11];
+  std::vector<uint32_t> large;
+  for (size_t i = 0; i < count; ++i) {
+    const bntt_job& jb = jobs[i];
+    BNTT_REQUIRE(jb.plan < b->plans.size(), "job %zu: plan index %u out of range", i, jb.plan);
+    BNTT_REQUIRE(jb.x && jb.y, "job %zu: NULL buffer", i);
+    BNTT_REQUIRE((((uintptr_t)jb.x | (uintptr_t)jb.y) & 15) == 0, "job %zu: buffers must be 16-byte aligned", i);
+    const bntt_plan* p = b->plans[jb.plan];
+    DevJob& d = sc.djobs[i];
+    d.x = static_cast<const uint4*>(jb.x);
+    d.y = static_cast<uint4*>(jb.y);
+    d.tw = static_cast<const uint4*>(p->tw);
+    d.log2n = p->log2n;
+    d.slot = 0;
+    if (p->log2n <= 10) {
+      by_size[p->log2n].push_back((uint32_t)i);
+    } else {
+      d.slot = (uint32_t)sc.nslots++;
+      large.push_back((uint32_t)i);
+    }
+  }
+  std::vector<WorkItem> later[kMaxPasses];
+  sc.pass_tiles.assign(sc.nslots * kMaxPasses, 0);
+  for (uint32_t ji : large) {
+    const DevJob& d = sc.djobs[ji];
+    const int n = (int)d.log2n;
+    const std::vector<int> passes = split_passes(n);
+    BNTT_REQUIRE(passes.size() <= (size_t)kMaxPasses, "log2n %d needs too many passes", n);
+    int s0 = 0;
+    for (size_t p = 0; p < passes.size(); ++p) {
+      const int m = passes[p];
+      const int l = n - s0 - m;
+      const int shape = l > 0 ? b->shapes.pass_il[m] : b->shapes.pass_contig[m];
+      BNTT_REQUIRE(shape >= 0, "no batch shape for pass m=%d", m);
+      const uint32_t tpc = (uint32_t)kShapes[shape].tpc;
+      const uint64_t nsub = 1ull << (n - m);
+      const uint32_t tiles = (uint32_t)((nsub + tpc - 1) / tpc);
+      sc.pass_tiles[d.slot * kMaxPasses + p] = tiles;
+      for (uint32_t t = 0; t < tiles; ++t) {
+        WorkItem w{};
+        w.shape = (uint16_t)shape;
+        w.kind = ITEM_PASS;
+        w.a = ji;
+        w.b = t * tpc;
+        w.pass = (uint16_t)p;
+        w.wait = p > 0 ? 1 : 0;
+        later[p].push_back(w);
+      }
+      s0 += m;
+    }
+  }
+  // queue: first passes, small tiles (largest size first), later passes
+  for (const WorkItem& w : later[0]) sc.items.push_back(w);
+  for (int n = 10; n >= 1; --n) {
+    const std::vector<uint32_t>& v = by_size[n];
+    if (v.empty()) continue;
+    const int shape = b->shapes.small[n];
+    BNTT_REQUIRE(shape >= 0, "no batch shape for size 2^%d", n);
+    const uint32_t tpc = (uint32_t)kShapes[shape].tpc;
+    const uint32_t base = (uint32_t)sc.order.size();
+    sc.order.insert(sc.order.end(), v.begin(), v.end());
+    for (uint32_t s = 0; s < v.size(); s += tpc) {
+      WorkItem w{};
+      w.shape = (uint16_t)shape;
+      w.kind = ITEM_SMALL;
+      w.a = base + s;
+      w.b = std::min<uint32_t>(tpc, (uint32_t)v.size() - s);
+      sc.items.push_back(w);
+    }
+  }
+  for (int p = 1; p < kMaxPasses; ++p)
+    for (const WorkItem& w : later[p]) sc.items.push_back(w);
+  return BNTT_OK;
+}
+
+// Copies the schedule to the device and captures [memset control words,
+// kernel] into a graph on `stream`.
+static int upload_and_capture(bntt_batch* b, Schedule& sc, cudaStream_t stream) {
+  bntt_ctx* c = b->ctx;
+  const size_t jb = sc.djobs.size() * sizeof(DevJob), ob = sc.order.size() * 4,
+               ib = sc.items.size() * sizeof(WorkItem), cb = (kCtlHeader + sc.nslots * kMaxPasses) * 4,
+               pb = sc.pass_tiles.size() * 4;
+  int rc;
+  if ((rc = grow(c, &sc.d_jobs, &sc.d_jobs_cap, jb)) || (rc = grow(c, &sc.d_order, &sc.d_order_cap, ob)) ||
+      (rc = grow(c, &sc.d_items, &sc.d_items_cap, ib)) || (rc = grow(c, &sc.d_ctl, &sc.d_ctl_cap, cb)) ||
+      (rc = grow(c, &sc.d_pass_tiles, &sc.d_pass_tiles_cap, pb)))
+    return rc;
+  if (jb) BNTT_CK(cudaMemcpyAsync(sc.d_jobs, sc.djobs.data(), jb, cudaMemcpyHostToDevice, stream));
+  if (ob) BNTT_CK(cudaMemcpyAsync(sc.d_order, sc.order.data(), ob, cudaMemcpyHostToDevice, stream));
+  if (ib) BNTT_CK(cudaMemcpyAsync(sc.d_items, sc.items.data(), ib, cudaMemcpyHostToDevice, stream));
+  if (pb) BNTT_CK(cudaMemcpyAsync(sc.d_pass_tiles, sc.pass_tiles.data(), pb, cudaMemcpyHostToDevice, stream));
+  BNTT_CK(cudaStreamSynchronize(stream));
+  if (sc.exec) {
+    cudaGraphExecDestroy(sc.exec);
+    sc.exec = nullptr;
+  }
+  if (sc.items.empty()) return BNTT_OK;
+  const void* fn = batch_kernel(b->fast);
+  size_t smem = 0;
+  bool used[kNumShapes] = {};
+  for (const WorkItem& w : sc.items) used[w.shape] = true;
+  for (int s = 0; s < kNumShapes; ++s)
+    if (used[s]) smem = std::max(smem, shape_smem(s));
+  BNTT_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1)));
+  int bps = 0;
+  BNTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, kBatchThreads, smem));
+  if (bps < 1) return set_error(BNTT_ECUDA, "batch kernel does not fit on an SM (smem %zu)", smem);
+  sc.grid = (int)std::min<size_t>((size_t)bps * c->sms, sc.items.size());
+  sc.smem = smem;
+  BatchArgs ba;
+  ba.items = static_cast<const WorkItem*>(sc.d_items);
+  ba.nitems = (uint32_t)sc.items.size();
+  ba.jobs = static_cast<const DevJob*>(sc.d_jobs);
+  ba.order = static_cast<const uint32_t*>(sc.d_order);
+  ba.ctl = static_cast<uint32_t*>(sc.d_ctl);
+  ba.pass_tiles = static_cast<const uint32_t*>(sc.d_pass_tiles);
+  ModParams mp = b->mp;
+  int layout = b->layout;
+  void* args[] = {&ba, &mp, &layout};
+  cudaGraph_t graph = nullptr;
+  BNTT_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e1 = cudaMemsetAsync(sc.d_ctl, 0, cb, stream);
+  cudaError_t e2 = cudaLaunchKernel(fn, dim3(sc.grid), dim3(kBatchThreads), args, smem, stream);
+  cudaError_t e3 = cudaStreamEndCapture(stream, &graph);
+  if (e1 != cudaSuccess) return cuda_error(e1, "cudaMemsetAsync(capture)");
+  if (e2 != cudaSuccess) return cuda_error(e2, "cudaLaunchKernel(capture)");
+  if (e3 != cudaSuccess) return cuda_error(e3, "cudaStreamEndCapture");
+  cudaError_t e4 = cudaGraphInstantiate(&sc.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e4 != cudaSuccess) return cuda_error(e4, "cudaGraphInstantiate");
+  sc.exec_stream = stream;
+  return BNTT_OK;
+}
+
+static int launch_schedule(bntt_batch* b, Schedule& sc, cudaStream_t stream) {
+  if (!sc.exec) return BNTT_OK;
+  BNTT_CK(cudaGraphLaunch(sc.exec, stream));
+  b->ctx->launches++;
+  b->last_launches++;
+  return BNTT_OK;
+}
+
+static int schedule_status(Schedule& sc) {
+  if (!sc.d_ctl) return BNTT_OK;
+  uint32_t err = 0;
+  BNTT_CK(cudaMemcpy(&err, static_cast<uint32_t*>(sc.d_ctl) + 1, 4, cudaMemcpyDeviceToHost));
+  if (err) return set_error(BNTT_ETIMEOUT, "a pass of a large transform waited too long for its predecessor");
+  return BNTT_OK;
+}
+
+}  // namespace bntt
+
+extern "C" {
+
+int bntt_batch_create(bntt_ctx* c, bntt_batch** out, bntt_plan* const* plans, size_t nplans) {
+  BNTT_REQUIRE(c && out && plans && nplans > 0, "NULL argument");
+  *out = nullptr;
+  for (size_t i = 0; i < nplans; ++i) {
+    BNTT_REQUIRE(plans[i] && plans[i]->ctx == c, "plan %zu is NULL or from another context", i);
+    BNTT_REQUIRE(memcmp(&plans[i]->mod, &plans[0]->mod, sizeof(bntt_modulus)) == 0 &&
+                     plans[i]->layout == plans[0]->layout,
+                 "all plans of a batch must share modulus and layout");
+  }
+  if (int rc = ctx_use_device(c)) return rc;
+  auto* b = new bntt_batch();
+  b->ctx = c;
+  b->plans.assign(plans, plans + nplans);
+  b->mp = plans[0]->mp;
+  b->fast = arith_fast(c, plans[0]->fast);
+  b->layout = plans[0]->layout;
+  for (int m = 0; m <= 10; ++m) {
+    b->shapes.small[m] = batch_shape_for(m, MAP_CONTIG, 0);
+    b->shapes.pass_il[m] = batch_shape_for(m, MAP_INTERLEAVED, 0);
+    b->shapes.pass_contig[m] = batch_shape_for(m, MAP_CONTIG, 4);
+    if (b->shapes.pass_contig[m] < 0) b->shapes.pass_contig[m] = batch_shape_for(m, MAP_CONTIG, 0);
+  }
+  *out = b;
+  return BNTT_OK;
+}
+
+int bntt_batch_destroy(bntt_batch* b) {
+  if (!b) return BNTT_OK;
+  bntt_ctx* c = b->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (int s = 0; s < 2; ++s) cudaStreamSynchronize(c->copy_stream[s]);
+  free_schedule(c, b->main);
+  for (Schedule& s : b->groups) free_schedule(c, s);
+  if (b->region) ctx_free(c, b->region);
+  delete b;
+  return BNTT_OK;
+}
+
+int bntt_batch_run_dev(bntt_batch* b, const bntt_job* jobs, size_t count) {
+  BNTT_REQUIRE(b && (jobs || count == 0), "NULL argument");
+  if (int rc = ctx_use_device(b->ctx)) return rc;
+  b->last_launches = 0;
+  if (count == 0) return BNTT_OK;
+  const bool same = b->last_jobs.size() == count && b->main.exec_stream == b->ctx->stream &&
+                    memcmp(b->last_jobs.data(), jobs, count * sizeof(bntt_job)) == 0;
+  if (!same) {
+    b->last_jobs.clear();
+    if (int rc = build_schedule(b, b->main, jobs, count)) return rc;
+    if (int rc = upload_and_capture(b, b->main, b->ctx->stream)) return rc;
+    b->last_jobs.assign(jobs, jobs + count);
+  }
+  return launch_schedule(b, b->main, b->ctx->stream);
+}
+
+int bntt_batch_status(bntt_batch* b) {
+  BNTT_REQUIRE(b, "NULL batch");
+  if (int rc = ctx_use_device(b->ctx)) return rc;
+  BNTT_CK(cudaStreamSynchronize(b->ctx->stream));
+  if (int rc = schedule_status(b->main)) return rc;
+  for (Schedule& s : b->groups)
+    if (int rc = schedule_status(s)) return rc;
+  return BNTT_OK;
+}
+
+size_t bntt_batch_last_launches(bntt_batch* b) { return b ? b->last_launches : 0; }
+
+// Host buffers: jobs are packed into one device region (in place), split into
+// groups of about 1/8 of the bytes each.  Group g's inputs go up on one copy
+// stream, its graph runs on the context stream, its outputs come back on the
+// other copy stream, so transfers of neighbouring groups overlap each other
+// and the kernels.  Host copies of jobs adjacent in host memory are merged.
+// Schedules and graphs are cached while the job list stays the same.
+int bntt_batch_run_host(bntt_batch* b, const bntt_job* jobs, size_t count) {
+  BNTT_REQUIRE(b && (jobs || count == 0), "NULL argument");
+  bntt_ctx* c = b->ctx;
+  if (int rc = ctx_use_device(c)) return rc;
+  b->last_launches = 0;
+  if (count == 0) return BNTT_OK;
+  cudaStream_t s_in = c->copy_stream[0], s_out = c->copy_stream[1], s_run = c->stream;
+  const bool same = b->host_last_jobs.size() == count &&
+                    memcmp(b->host_last_jobs.data(), jobs, count * sizeof(bntt_job)) == 0;
+  for (size_t i = 0; i < count && !same; ++i) {
+    BNTT_REQUIRE(jobs[i].plan < b->plans.size(), "job %zu: plan index out of range", i);
+    BNTT_REQUIRE(jobs[i].x && jobs[i].y, "job %zu: NULL buffer", i);
+  }
+  auto bytes_of = [&](size_t i) { return (size_t)16 << b->plans[jobs[i].plan]->log2n; };
+  if (!same) {
+    b->host_last_jobs.clear();
+    size_t total = 0;
+    b->dev_off.assign(count, 0);
+    for (size_t i = 0; i < count; ++i) {
+      b->dev_off[i] = total;
+      total += bytes_of(i);
+    }
+    if (int rc = grow(c, &b->region, &b->region_cap, total)) return rc;
+    const size_t target = std::max<size_t>(total / 8, 16u << 20);
+    b->group_first.clear();
+    b->group_first.push_back(0);
+    size_t acc = 0;
+    for (size_t i = 0; i < count; ++i) {
+      acc += bytes_of(i);
+      if (acc >= target && i + 1 < count) {
+        b->group_first.push_back(i + 1);
+        acc = 0;
+      }
+    }
+    b->group_first.push_back(count);
+    const size_t ng = b->group_first.size() - 1;
+    for (size_t g = ng; g < b->groups.size(); ++g) free_schedule(c, b->groups[g]);
+    b->groups.resize(ng);
+    std::vector<bntt_job> dj(jobs, jobs + count);
+    for (size_t i = 0; i < count; ++i) {
+      void* p = static_cast<char*>(b->region) + b->dev_off[i];
+      dj[i].x = p;
+      dj[i].y = p;
+    }
+    for (size_t g = 0; g < ng; ++g) {
+      const size_t f = b->group_first[g], e = b->group_first[g + 1];
+      if (int rc = build_schedule(b, b->groups[g], dj.data() + f, e - f)) return rc;
+      if (int rc = upload_and_capture(b, b->groups[g], s_run)) return rc;
+    }
+    b->host_last_jobs.assign(jobs, jobs + count);
+  }
+  // work queued earlier on the context stream comes first
+  BNTT_CK(cudaEventRecord(c->ev[0], s_run));
+  BNTT_CK(cudaStreamWaitEvent(s_in, c->ev[0], 0));
+  BNTT_CK(cudaStreamWaitEvent(s_out, c->ev[0], 0));
+  char* region = static_cast<char*>(b->region);
+  const size_t ng = b->groups.size();
+  for (size_t g = 0; g < ng; ++g) {
+    const size_t f = b->group_first[g], e = b->group_first[g + 1];
+    for (size_t i = f; i < e;) {  // merged input copies
+      size_t j = i + 1, run = bytes_of(i);
+      while (j < e && static_cast<const char*>(jobs[j].x) == static_cast<const char*>(jobs[i].x) + run) {
+        run += bytes_of(j);
+        ++j;
+      }
+      BNTT_CK(cudaMemcpyAsync(region + b->dev_off[i], jobs[i].x, run, cudaMemcpyHostToDevice, s_in));
+      i = j;
+    }
+    cudaEvent_t in_done = c->ev[1 + (g % 3)], run_done = c->ev[4 + (g % 3)];
+    BNTT_CK(cudaEventRecord(in_done, s_in));
+    BNTT_CK(cudaStreamWaitEvent(s_run, in_done, 0));
+    if (int rc = launch_schedule(b, b->groups[g], s_run)) return rc;
+    BNTT_CK(cudaEventRecord(run_done, s_run));
+    BNTT_CK(cudaStreamWaitEvent(s_out, run_done, 0));
+    for (size_t i = f; i < e;) {  // merged output copies
+      size_t j = i + 1, run = bytes_of(i);
+      while (j < e && static_cast<char*>(jobs[j].y) == static_cast<char*>(jobs[i].y) + run) {
+        run += bytes_of(j);
+        ++j;
+      }
+      BNTT_CK(cudaMemcpyAsync(jobs[i].y, region + b->dev_off[i], run, cudaMemcpyDeviceToHost, s_out));
+      i = j;
+    }
+  }
+  BNTT_CK(cudaStreamSynchronize(s_in));
+  BNTT_CK(cudaStreamSynchronize(s_run));
+  BNTT_CK(cudaStreamSynchronize(s_out));
+  for (Schedule& s : b->groups)
+    if (int rc = schedule_status(s)) return rc;
+  return BNTT_OK;
+}
+
+}  // extern "C"
+
+// The plain per-call path over the same job list: every job is its own
+// forward transform, launched separately (one launch per transform of at most
+// 1024 points, one per HBM pass above).  This is the comparison point of the
+// persistent kernel, issued from C so that only launch cost is measured.
+extern "C" int bntt_batch_run_percall_dev(bntt_batch* b, const bntt_job* jobs, size_t count) {
+  BNTT_REQUIRE(b && (jobs || count == 0), "NULL argument");
+  if (int rc = ctx_use_device(b->ctx)) return rc;
+  b->last_launches = 0;
+  const uint64_t before = b->ctx->launches;
+  for (size_t i = 0; i < count; ++i) {
+    BNTT_REQUIRE(jobs[i].plan < b->plans.size(), "job %zu: plan index out of range", i);
+    BNTT_REQUIRE(jobs[i].x && jobs[i].y && (((uintptr_t)jobs[i].x | (uintptr_t)jobs[i].y) & 15) == 0,
+                 "job %zu: NULL or misaligned buffer", i);
+    if (int rc = ntt_forward_on(b->plans[jobs[i].plan], jobs[i].y, jobs[i].x, 1, b->ctx->stream)) return rc;
+  }
+  b->last_launches = (size_t)(b->ctx->launches - before);
+  return BNTT_OK;
+}

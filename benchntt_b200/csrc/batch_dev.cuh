@@ -1,0 +1,199 @@
+// batch_dev.cuh -- device side of the batch engine: many independent transforms of uneven sizes in one persistent,
+// graph-launched work-queue kernel.
+//
+// Work items (16 bytes each) are tiles of 256 threads:
+//   SMALL   TPC transforms of one size 2^n <= 1024, taken from a list of
+//           jobs sorted by size (one sub-transform per job)
+//   PASS p  TPC sub-transforms of HBM pass p of one large transform
+//           (n > 10, passes from split_passes: e.g. 2^20 = 10 + 10)
+// A CTA takes the next item with an atomic counter.  Queue order is: all
+// first passes of large jobs, then small tiles from the largest size down,
+// then later passes.  Pass p > 0 of a job reads what pass p-1 wrote, so its
+// tiles first wait until the job's pass p-1 counter reaches that pass's tile
+// count.  The wait cannot deadlock: every pass p-1 tile was handed out
+// before any pass p tile and its CTA finishes it without waiting.  The wait is
+// still bounded; when it gives up it raises the error word, the tile is
+// skipped, and bntt_batch_status() reports BNTT_ETIMEOUT.
+//
+// The control words (queue head, error word, per-job pass counters) live in a
+// device workspace owned by the batch and are cleared by a memset node of the
+// same CUDA graph before each launch.
+#pragma once
+#include "internal.h"
+#include "ntt_core.cuh"
+
+namespace bntt {
+
+constexpr int kBatchThreads = 256;
+
+struct DevJob {
+  const uint4* x;
+  uint4* y;
+  const uint4* tw;
+  uint32_t log2n;
+  uint32_t slot;  // counter slot for large jobs
+};
+
+enum : uint32_t { ITEM_SMALL = 0, ITEM_PASS = 1 };
+
+struct WorkItem {
+  uint16_t shape;   // index into the shape table below
+  uint16_t kind;    // ITEM_SMALL or ITEM_PASS
+  uint32_t a;       // SMALL: first position in the size-sorted order; PASS: job index
+  uint32_t b;       // SMALL: number of jobs in the tile; PASS: first sub-transform id
+  uint16_t pass;    // PASS: pass index
+  uint16_t wait;    // PASS: 1 if the tile waits for the previous pass
+};
+static_assert(sizeof(WorkItem) == 16, "work item layout");
+
+// Shapes available to the persistent kernel: all have 256 threads.
+#define BNTT_BATCH_SHAPES(X)               \
+  X(0, 1, 1, 256, MAP_CONTIG)              \
+  X(1, 2, 2, 256, MAP_CONTIG)              \
+  X(2, 3, 3, 256, MAP_CONTIG)              \
+  X(3, 4, 4, 256, MAP_CONTIG)              \
+  X(4, 5, 3, 64, MAP_CONTIG)               \
+  X(5, 6, 3, 32, MAP_CONTIG)               \
+  X(6, 7, 3, 16, MAP_CONTIG)               \
+  X(7, 8, 3, 8, MAP_CONTIG)                \
+  X(8, 9, 3, 4, MAP_CONTIG)                \
+  X(9, 10, 3, 2, MAP_CONTIG)               \
+  X(10, 5, 4, 128, MAP_CONTIG)             \
+  X(11, 6, 4, 64, MAP_CONTIG)              \
+  X(12, 7, 4, 32, MAP_CONTIG)              \
+  X(13, 8, 4, 16, MAP_CONTIG)              \
+  X(14, 9, 4, 8, MAP_CONTIG)               \
+  X(15, 10, 4, 4, MAP_CONTIG)              \
+  X(16, 5, 4, 128, MAP_INTERLEAVED)        \
+  X(17, 6, 4, 64, MAP_INTERLEAVED)         \
+  X(18, 7, 4, 32, MAP_INTERLEAVED)         \
+  X(19, 8, 4, 16, MAP_INTERLEAVED)         \
+  X(20, 9, 4, 8, MAP_INTERLEAVED)          \
+  X(21, 10, 4, 4, MAP_INTERLEAVED)
+
+struct BatchShape {
+  int m, logr, tpc, map;
+};
+inline constexpr BatchShape kShapes[] = {
+#define BNTT_SHAPE_ROW(id, M, LOGR, TPC, MAP) {M, LOGR, TPC, MAP},
+    BNTT_BATCH_SHAPES(BNTT_SHAPE_ROW)
+#undef BNTT_SHAPE_ROW
+};
+constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+
+// control words: [0] queue head, [1] error word, [2 + 4*slot + p] pass counters
+constexpr int kCtlHeader = 2;
+constexpr int kMaxPasses = 4;
+// bounded wait: polls x ~100 ns sleeps, several seconds in all
+constexpr uint32_t kWaitPolls = 1u << 25;
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+struct BatchArgs {
+  const WorkItem* items;
+  uint32_t nitems;
+  const DevJob* jobs;
+  const uint32_t* order;   // job indices sorted by size (SMALL tiles)
+  uint32_t* ctl;
+  const uint32_t* pass_tiles;  // [slot * kMaxPasses + p] tile count of pass p
+};
+
+// One device function per shape (not inlined into the kernel's switch): keeps
+// ptxas compile time linear in the number of shapes.
+template <int M, int LOGR, int TPC, int MAP, class Arith>
+__device__ __noinline__ void run_item(const WorkItem& it, const BatchArgs& ba, uint4* smem,
+                                         const ModParams& mp, int layout, int* s_flag) {
+  using T = NttTile<M, LOGR, TPC, MAP, Arith>;
+  static_assert(T::THREADS == kBatchThreads, "batch shapes use 256 threads");
+  const int tid = threadIdx.x;
+  const int sub = T::sub_of(tid), lane = T::lane_of(tid);
+  if (it.kind == ITEM_SMALL) {
+    SubRef sr;
+    sr.valid = (uint32_t)sub < it.b;
+    const DevJob& j = ba.jobs[ba.order[it.a + (sr.valid ? (uint32_t)sub : 0u)]];
+    sr.x = j.x;
+    sr.y = j.y;
+    sr.tw = j.tw;
+    sr.trow = 1;
+    sr.lshift = 0;
+    T::template run<LD_NC>(sr, sub, lane, smem, mp, layout);
+    return;
+  }
+  const DevJob& j = ba.jobs[it.a];
+  // pass geometry of this job (same split as split_passes on the host)
+  const int n = (int)j.log2n;
+  const int k = (n + 9) / 10;
+  int s0 = 0;
+  for (int p = 0; p < (int)it.pass; ++p) s0 += n / k + (p < n % k ? 1 : 0);
+  SubGeom g;
+  g.x = it.pass == 0 ? j.x : j.y;
+  g.y = j.y;
+  g.tw = j.tw;
+  g.n = (uint32_t)n;
+  g.s0 = (uint32_t)s0;
+  g.m = (uint32_t)M;
+  g.l = (uint32_t)(n - s0 - M);
+  g.nsub = 1ull << (n - M);
+  uint32_t* counters = ba.ctl + kCtlHeader + j.slot * kMaxPasses;
+  if (it.wait) {
+    if (tid == 0) {
+      const uint32_t want = ba.pass_tiles[j.slot * kMaxPasses + it.pass - 1];
+      uint32_t polls = 0;
+      int ok = 1;
+      while (ld_acquire(&counters[it.pass - 1]) < want) {
+        if (++polls > kWaitPolls) {
+          atomicOr(&ba.ctl[1], 1u);
+          ok = 0;
+          break;
+        }
+        __nanosleep(100);
+      }
+      *s_flag = ok;
+    }
+    __syncthreads();
+    if (!*s_flag) {
+      __syncthreads();
+      return;
+    }
+  }
+  const SubRef sr = make_subref(g, (uint64_t)it.b + (uint64_t)sub);
+  if (it.pass == 0) T::template run<LD_NC>(sr, sub, lane, smem, mp, layout);
+  else T::template run<LD_CG>(sr, sub, lane, smem, mp, layout);
+  // publish this tile: every thread's stores, then one release increment
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    atomicAdd(&counters[it.pass], 1u);
+  }
+}
+
+template <class Arith>
+__global__ void __launch_bounds__(kBatchThreads) k_batch(BatchArgs ba, ModParams mp, int layout) {
+  extern __shared__ uint4 smem[];
+  __shared__ uint32_t s_item;
+  __shared__ int s_flag;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(&ba.ctl[0], 1u);
+    __syncthreads();
+    const uint32_t i = s_item;
+    if (i >= ba.nitems) break;
+    const WorkItem it = ba.items[i];
+    switch (it.shape) {
+#define BNTT_SHAPE_CASE(id, M, LOGR, TPC, MAP)                                  \
+  case id:                                                                      \
+    run_item<M, LOGR, TPC, MAP, Arith>(it, ba, smem, mp, layout, &s_flag);      \
+    break;
+      BNTT_BATCH_SHAPES(BNTT_SHAPE_CASE)
+#undef BNTT_SHAPE_CASE
+      default:
+        break;
+    }
+    __syncthreads();  // smem and s_item are reused by the next item
+  }
+}
+
+}  // namespace bntt

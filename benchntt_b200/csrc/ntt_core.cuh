@@ -1,0 +1,209 @@
+// ntt_core.cuh -- the forward network of benchNTT on sm_100a.
+//
+// The reference transform (src/ntt_scalar.c:582-627) is a radix-2 network:
+// with n = log2 N, stage s (0 <= s < n) pairs indices that differ in bit
+// n-1-s and multiplies by the table entry T[2^s + (index >> (n - s))].  The
+// reference evaluates it in constant-geometry order with ping-pong buffers;
+// here it is evaluated in place, in natural order, which yields the same
+// outputs (tests check both against the reference).
+//
+// Sub-transforms.  Stages [S0, S0 + M) of an n-point transform touch index
+// bits [L, L + M) with L = n - S0 - M; every assignment of the other bits --
+// the top S0 bits H and the low L bits c -- selects an independent 2^M-point
+// sub-network on the elements
+//     idx(j) = (H << (n - S0)) | (j << L) | c,     j in [0, 2^M)
+// whose stage S0 + s multiplies by
+//     T[((2^S0 + H) << s) + (j >> (M - s))].
+// A small transform is one sub-transform (S0 = L = 0).  Large transforms run
+// as passes over HBM: for 2^20, pass A has S0 = 0, M = 10, L = 10 (columns)
+// and pass B has S0 = 10, M = 10, L = 0 (rows).  This holds for any table T
+// because it only regroups the network's data flow.
+//
+// Inside a sub-transform each thread holds R = 2^LOGR elements in registers.
+// The M stages are cut into passes of at most LOGR stages; in a pass a thread
+// owns R / 2^r groups of 2^r elements that differ only in that pass's bits
+// and runs the r stages on them without communication.  Passes exchange data
+// through shared memory (XOR-swizzled 16-byte slots), the first pass reads
+// HBM and the last writes HBM.
+#pragma once
+#include "u128.cuh"
+
+namespace bntt {
+
+enum : int { MAP_CONTIG = 0, MAP_INTERLEAVED = 1 };
+
+// Where one sub-transform's elements and twiddles live, as a thread sees it.
+struct SubRef {
+  const uint4* x;    // element j at x[j << L]
+  uint4* y;          // element j at y[j << L]
+  const uint4* tw;   // table of the whole transform
+  uint32_t trow;     // 2^S0 + H
+  uint32_t lshift;   // L
+  bool valid;
+};
+
+// Load policy for the first pass's HBM reads: the read-only path, or L2 only
+// (coherent with writes made earlier in the same kernel by other CTAs).
+enum : int { LD_NC = 0, LD_CG = 1 };
+
+template <int LDP>
+__device__ __forceinline__ uint4 ld_data(const uint4* p) {
+  if constexpr (LDP == LD_CG) return __ldcg(p);
+  else return __ldg(p);
+}
+
+template <int M, int LOGR, int TPC, int MAP, class Arith>
+struct NttTile {
+  static constexpr int R = 1 << LOGR;
+  static constexpr int N = 1 << M;
+  static constexpr int TPT = N / R;             // threads per sub-transform
+  static constexpr int THREADS = TPC * TPT;
+  static constexpr int NPASS = (M + LOGR - 1) / LOGR;
+  static constexpr int PBASE = M / NPASS, PEXTRA = M % NPASS;
+  static constexpr int SMEM_SLOTS = NPASS > 1 ? TPC * N : 0;
+  // a sub-transform's threads sit in one warp
+  static constexpr bool WARP_LOCAL = (MAP == MAP_CONTIG) && (TPT <= 32);
+  static_assert(M >= 1 && LOGR >= 1 && LOGR <= M, "bad shape");
+
+  __host__ __device__ static constexpr int bits(int p) { return PBASE + (p < PEXTRA ? 1 : 0); }
+  __host__ __device__ static constexpr int start(int p) {
+    return p * PBASE + (p < PEXTRA ? p : PEXTRA);
+  }
+
+  __device__ __forceinline__ static int sub_of(int tid) {
+    return MAP == MAP_INTERLEAVED ? tid % TPC : tid / TPT;
+  }
+  __device__ __forceinline__ static int lane_of(int tid) {
+    return MAP == MAP_INTERLEAVED ? tid / TPC : tid % TPT;
+  }
+
+  // shared-memory slot of element j of sub-transform `sub`
+  __device__ __forceinline__ static int slot(int sub, int j) {
+    if constexpr (MAP == MAP_INTERLEAVED) {
+      return j * TPC + sub;
+    } else {
+      const int sw = (M >= 3) ? (j ^ ((j >> 3) & 7)) : j;
+      return (sub << M) | sw;
+    }
+  }
+
+  __device__ __forceinline__ static void sync() {
+    if constexpr (WARP_LOCAL) __syncwarp();
+    else __syncthreads();
+  }
+
+  // Runs the whole sub-transform.  Every thread of the tile must call it
+  // (it synchronises); threads whose sub-transform is not valid compute on
+  // zeros and store nothing.
+  template <int LDP>
+  __device__ __forceinline__ static void run(const SubRef& sr, int sub, int lane, uint4* smem,
+                                             const ModParams& mp, int layout) {
+    U128 v[R];
+    pass<0, LDP>(v, sr, sub, lane, smem, mp, layout);
+  }
+
+  template <int P, int LDP>
+  __device__ __forceinline__ static void pass(U128 (&v)[R], const SubRef& sr, int sub, int lane,
+                                              uint4* smem, const ModParams& mp, int layout) {
+    constexpr int r = bits(P);
+    constexpr int s0 = start(P);
+    constexpr int lo = M - s0 - r;        // lowest local bit this pass touches
+    constexpr int G = 1 << r;             // elements per group
+    constexpr int GPT = R / G;            // groups per thread
+    static_assert(GPT >= 1, "pass wider than the register tile");
+
+    // ---- gather
+#pragma unroll
+    for (int i = 0; i < GPT; ++i) {
+      const int g = lane + i * TPT;
+      const int base = (g & ((1 << lo) - 1)) | ((g >> lo) << (lo + r));
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const int idx = base | (j << lo);
+        if constexpr (P == 0) {
+          if (sr.valid) {
+            v[i * G + j] = from_mem(ld_data<LDP>(sr.x + ((size_t)idx << sr.lshift)), layout);
+          } else {
+#pragma unroll
+            for (int w = 0; w < 4; ++w) v[i * G + j].w[w] = 0u;
+          }
+        } else {
+          const uint4 t = smem[slot(sub, idx)];
+          v[i * G + j] = U128{{t.x, t.y, t.z, t.w}};
+        }
+      }
+    }
+
+    // ---- r stages on each group
+#pragma unroll
+    for (int i = 0; i < GPT; ++i) {
+      const int g = lane + i * TPT;
+      const uint32_t gt = (sr.trow << s0) + (uint32_t)(g >> lo);
+#pragma unroll
+      for (int t = 0; t < r; ++t) {
+        const int half = 1 << (r - 1 - t);
+#pragma unroll
+        for (int u = 0; u < (1 << t); ++u) {
+          const U128 w = from_mem(__ldg(sr.tw + ((gt << t) + (uint32_t)u)), layout);
+#pragma unroll
+          for (int k = 0; k < half; ++k) {
+            const int j = (u << (r - t)) | k;
+            butterfly<Arith>(v[i * G + j], v[i * G + j + half], w, mp);
+          }
+        }
+      }
+    }
+
+    // ---- scatter
+#pragma unroll
+    for (int i = 0; i < GPT; ++i) {
+      const int g = lane + i * TPT;
+      const int base = (g & ((1 << lo) - 1)) | ((g >> lo) << (lo + r));
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const int idx = base | (j << lo);
+        if constexpr (P == NPASS - 1) {
+          if (sr.valid) sr.y[(size_t)idx << sr.lshift] = to_mem(v[i * G + j], layout);
+        } else {
+          const U128& e = v[i * G + j];
+          smem[slot(sub, idx)] = make_uint4(e.w[0], e.w[1], e.w[2], e.w[3]);
+        }
+      }
+    }
+    if constexpr (P + 1 < NPASS) {
+      sync();
+      pass<P + 1, LDP>(v, sr, sub, lane, smem, mp, layout);
+    }
+  }
+};
+
+// Geometry of one launch over sub-transforms (see the header comment).
+struct SubGeom {
+  const uint4* x;
+  uint4* y;
+  const uint4* tw;
+  uint32_t n;       // log2 of the whole transform
+  uint32_t s0;      // first stage of this pass
+  uint32_t m;       // stages in this pass
+  uint32_t l;       // low bits below the pass bits
+  uint64_t nsub;    // number of sub-transforms (all transforms of the batch)
+};
+
+// Sub-transform `sid` of a geometry: sid = (transform << (S0 + L)) | (H << L) | c.
+__device__ __forceinline__ SubRef make_subref(const SubGeom& g, uint64_t sid) {
+  SubRef r;
+  r.valid = sid < g.nsub;
+  const uint64_t s = r.valid ? sid : 0;
+  const uint64_t big = s >> (g.s0 + g.l);
+  const uint64_t hbits = (s >> g.l) & ((1ull << g.s0) - 1);
+  const uint64_t c = s & ((1ull << g.l) - 1);
+  const uint64_t off = (big << g.n) + (hbits << (g.n - g.s0)) + c;
+  r.x = g.x + off;
+  r.y = g.y + off;
+  r.tw = g.tw;
+  r.trow = (1u << g.s0) + (uint32_t)hbits;
+  r.lshift = g.l;
+  return r;
+}
+
+}  // namespace bntt

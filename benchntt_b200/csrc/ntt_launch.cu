@@ -1,0 +1,133 @@
+// ntt_launch.cu -- registry of compiled sub-transform kernels, the HBM pass
+// split, and the stream-ordered forward transform.
+#include <algorithm>
+#include <mutex>
+
+#include "internal.h"
+#include "ntt_core.cuh"
+
+namespace bntt {
+
+void append_fast_contig(std::vector<SubKernel>& v);
+void append_fast_contig_r4(std::vector<SubKernel>& v);
+void append_fast_il(std::vector<SubKernel>& v);
+void append_ref(std::vector<SubKernel>& v);
+
+const std::vector<SubKernel>& sub_kernels() {
+  static std::vector<SubKernel> v = [] {
+    std::vector<SubKernel> r;
+    append_fast_contig(r);
+    append_fast_contig_r4(r);
+    append_fast_il(r);
+    append_ref(r);
+    return r;
+  }();
+  return v;
+}
+
+const SubKernel* pick_sub_kernel(int m, int map, int fast, int logr_pref, int tpc_pref) {
+  const SubKernel* best = nullptr;
+  for (const SubKernel& k : sub_kernels()) {
+    if (k.m != m || k.map != map || k.fast != fast) continue;
+    if (logr_pref && k.logr != logr_pref) continue;
+    if (tpc_pref && k.tpc != tpc_pref) continue;
+    if (!best) best = &k;  // the first registered shape is the default
+  }
+  return best;
+}
+
+int blocks_per_sm(const SubKernel* k) {
+  static std::mutex mu;
+  std::lock_guard<std::mutex> g(mu);
+  SubKernel* mk = const_cast<SubKernel*>(k);
+  if (mk->max_blocks_per_sm > 0) return mk->max_blocks_per_sm;
+  if (k->smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)k->smem);
+    if (e != cudaSuccess) return -cuda_error(e, "cudaFuncSetAttribute(smem)");
+  }
+  int b = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k->fn, k->threads, k->smem);
+  if (e != cudaSuccess) return -cuda_error(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (b < 1) return -set_error(BNTT_ECUDA, "kernel m=%d logr=%d tpc=%d does not fit on an SM", k->m,
+                               k->logr, k->tpc);
+  mk->max_blocks_per_sm = b;
+  return b;
+}
+
+int launch_sub(bntt_ctx* ctx, const SubKernel* k, const void* geom, const ModParams& mp,
+               int layout, cudaStream_t stream, int grid_cap) {
+  const SubGeom& g = *static_cast<const SubGeom*>(geom);
+  const uint64_t ntiles = (g.nsub + (uint64_t)k->tpc - 1) / (uint64_t)k->tpc;
+  if (ntiles == 0) return BNTT_OK;
+  const int bps = blocks_per_sm(k);
+  if (bps < 0) return -bps;
+  uint64_t grid = std::min<uint64_t>(ntiles, (uint64_t)bps * (uint64_t)ctx->sms);
+  if (grid_cap > 0) grid = std::min<uint64_t>(grid, (uint64_t)grid_cap);
+  SubGeom gg = g;
+  ModParams mm = mp;
+  int lay = layout;
+  void* args[] = {&gg, &mm, &lay};
+  BNTT_CK(cudaLaunchKernel(k->fn, dim3((unsigned)grid), dim3(k->threads), args, k->smem, stream));
+  ctx->launches++;
+  return BNTT_OK;
+}
+
+// Balanced split of n stages into HBM passes of at most 10 stages each
+// (a 2^10-point sub-transform is the largest that lives in one CTA).
+std::vector<int> split_passes(int n) {
+  std::vector<int> p;
+  const int k = (n + 9) / 10;
+  for (int i = 0; i < k; ++i) p.push_back(n / k + (i < n % k ? 1 : 0));
+  return p;
+}
+
+int plan_choose_kernels(bntt_plan* p) {
+  const int n = (int)p->log2n;
+  p->passes = split_passes(n);
+  p->kernels.clear();
+  const bool fast = arith_fast(p->ctx, p->fast);
+  int s0 = 0;
+  for (size_t i = 0; i < p->passes.size(); ++i) {
+    const int m = p->passes[i];
+    const int l = n - s0 - m;
+    const int map = l > 0 ? MAP_INTERLEAVED : MAP_CONTIG;
+    // the first registered shape that fits (interleaved tiles need TPC
+    // adjacent columns, so TPC <= 2^l)
+    const SubKernel* k = nullptr;
+    for (const SubKernel& c : sub_kernels()) {
+      if (c.m != m || c.map != map || c.fast != (fast ? 1 : 0)) continue;
+      if (map == MAP_INTERLEAVED && (1 << l) < c.tpc) continue;
+      k = &c;
+      break;
+    }
+    if (!k) return set_error(BNTT_EINVAL, "no kernel compiled for pass m=%d map=%d", m, map);
+    p->kernels.push_back(k);
+    s0 += m;
+  }
+  return BNTT_OK;
+}
+
+int ntt_forward_on(bntt_plan* plan, void* y, const void* x, size_t batch, cudaStream_t s) {
+  if (batch == 0) return BNTT_OK;
+  const int n = (int)plan->log2n;
+  int s0 = 0;
+  for (size_t i = 0; i < plan->passes.size(); ++i) {
+    const int m = plan->passes[i];
+    SubGeom g;
+    g.x = static_cast<const uint4*>(i == 0 ? x : y);
+    g.y = static_cast<uint4*>(y);
+    g.tw = static_cast<const uint4*>(plan->tw);
+    g.n = (uint32_t)n;
+    g.s0 = (uint32_t)s0;
+    g.m = (uint32_t)m;
+    g.l = (uint32_t)(n - s0 - m);
+    g.nsub = (uint64_t)batch << (n - m);
+    int rc = launch_sub(plan->ctx, plan->kernels[i], &g, plan->mp, plan->layout, s);
+    if (rc) return rc;
+    s0 += m;
+  }
+  return BNTT_OK;
+}
+
+}  // namespace bntt

@@ -1,0 +1,296 @@
+// u128.cuh -- 128-bit modular arithmetic on sm_100a for the benchNTT hot path.
+//
+// A residue is four little-endian 32-bit limbs (w[0] least significant).
+// In HBM an element is 16 bytes in one of two layouts:
+//   HILO : the reference's u64 pair, high word first (src/config.c:29-30);
+//          as u32 words: [hi.lo32, hi.hi32, lo.lo32, lo.hi32]
+//   U128 : a native little-endian unsigned __int128 (the scalar API's
+//          uint128_t arrays, src/ntt_scalar.c:582)
+//
+// Two multiply policies produce results bit-identical to the reference
+// mulmod128 (src/ntt_scalar.c:173-199):
+//   ArithFast -- q = 2^124 - k with k < 2^14 and mu = floor(2^251 / q) (both
+//     reference primes).  For such (q, mu) and operands below 2^124 the
+//     reference's Barrett quotient is within one of the true quotient, so its
+//     single conditional subtraction always lands in [0, q): the reference
+//     returns exactly a*b mod q.  ArithFast computes that value with a
+//     pseudo-Mersenne fold (2^124 == k mod q): 16 limb products for a*b, 4 for
+//     the first fold, 1 for the second, one conditional subtraction.
+//   ArithRef  -- every other (q, mu): a replica of the reference's 64-bit word
+//     data flow, including the points where it drops carries, so it matches
+//     for arbitrary 128-bit inputs.
+// add and sub are the reference's exact semantics in both policies,
+// including addmod's two corner behaviours (see addmod_ref).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bntt {
+
+struct U128 {
+  uint32_t w[4];
+};
+
+// Parameters of one modulus as the kernels see them.
+struct ModParams {
+  U128 q;        // modulus
+  U128 mu;       // Barrett constant of the reference (used by ArithRef)
+  uint32_t k;    // q = 2^124 - k (used by ArithFast)
+  uint32_t pad[3];
+};
+
+enum Layout : int { LAYOUT_HILO = 0, LAYOUT_U128 = 1 };
+
+__device__ __forceinline__ U128 from_mem(uint4 v, int layout) {
+  U128 r;
+  if (layout == LAYOUT_HILO) {
+    r.w[0] = v.z; r.w[1] = v.w; r.w[2] = v.x; r.w[3] = v.y;
+  } else {
+    r.w[0] = v.x; r.w[1] = v.y; r.w[2] = v.z; r.w[3] = v.w;
+  }
+  return r;
+}
+
+__device__ __forceinline__ uint4 to_mem(const U128& a, int layout) {
+  if (layout == LAYOUT_HILO) return make_uint4(a.w[2], a.w[3], a.w[0], a.w[1]);
+  return make_uint4(a.w[0], a.w[1], a.w[2], a.w[3]);
+}
+
+// ---------------------------------------------------------------- add / sub
+
+// Reference addmod128 (src/ntt_scalar.c:49-79).  s = a + b mod 2^128 and
+// e = q - s mod 2^128; the borrow out of e is "s > q" (a strict test, so
+// s == q is returned as q).  The reference assembles s - q from e's 64-bit
+// words as (~e.hi, -e.lo): equal to s - q except when lo64(s) == lo64(q),
+// where its high word comes out one lower.  This routine reproduces exactly
+// that.
+__device__ __forceinline__ U128 addmod_ref(const U128& a, const U128& b, const U128& q) {
+  uint32_t s0, s1, s2, s3, e0, e1, e2, e3, gt;
+  asm("add.cc.u32  %0, %9, %13;\n\t"
+      "addc.cc.u32 %1, %10, %14;\n\t"
+      "addc.cc.u32 %2, %11, %15;\n\t"
+      "addc.u32    %3, %12, %16;\n\t"
+      "sub.cc.u32  %4, %17, %0;\n\t"
+      "subc.cc.u32 %5, %18, %1;\n\t"
+      "subc.cc.u32 %6, %19, %2;\n\t"
+      "subc.cc.u32 %7, %20, %3;\n\t"
+      "subc.u32    %8, 0, 0;\n\t"
+      : "=&r"(s0), "=&r"(s1), "=&r"(s2), "=&r"(s3), "=&r"(e0), "=&r"(e1), "=&r"(e2),
+        "=&r"(e3), "=r"(gt)
+      : "r"(a.w[0]), "r"(a.w[1]), "r"(a.w[2]), "r"(a.w[3]), "r"(b.w[0]), "r"(b.w[1]),
+        "r"(b.w[2]), "r"(b.w[3]), "r"(q.w[0]), "r"(q.w[1]), "r"(q.w[2]), "r"(q.w[3]));
+  uint32_t n0, n1;
+  asm("sub.cc.u32 %0, 0, %2;\n\t"
+      "subc.u32   %1, 0, %3;\n\t"
+      : "=r"(n0), "=r"(n1)
+      : "r"(e0), "r"(e1));
+  U128 r;
+  const bool sub = gt != 0u;
+  r.w[0] = sub ? n0 : s0;
+  r.w[1] = sub ? n1 : s1;
+  r.w[2] = sub ? ~e2 : s2;
+  r.w[3] = sub ? ~e3 : s3;
+  return r;
+}
+
+// Reference submod128 (src/ntt_scalar.c:81-104): d = a - b, plus q on borrow.
+__device__ __forceinline__ U128 submod_ref(const U128& a, const U128& b, const U128& q) {
+  uint32_t d0, d1, d2, d3, bw;
+  asm("sub.cc.u32  %0, %5, %9;\n\t"
+      "subc.cc.u32 %1, %6, %10;\n\t"
+      "subc.cc.u32 %2, %7, %11;\n\t"
+      "subc.cc.u32 %3, %8, %12;\n\t"
+      "subc.u32    %4, 0, 0;\n\t"
+      : "=&r"(d0), "=&r"(d1), "=&r"(d2), "=&r"(d3), "=r"(bw)
+      : "r"(a.w[0]), "r"(a.w[1]), "r"(a.w[2]), "r"(a.w[3]), "r"(b.w[0]), "r"(b.w[1]),
+        "r"(b.w[2]), "r"(b.w[3]));
+  // add (q & borrow-mask): one chain, no select
+  uint32_t m0 = q.w[0] & bw, m1 = q.w[1] & bw, m2 = q.w[2] & bw, m3 = q.w[3] & bw;
+  U128 r;
+  asm("add.cc.u32  %0, %4, %8;\n\t"
+      "addc.cc.u32 %1, %5, %9;\n\t"
+      "addc.cc.u32 %2, %6, %10;\n\t"
+      "addc.u32    %3, %7, %11;\n\t"
+      : "=r"(r.w[0]), "=r"(r.w[1]), "=r"(r.w[2]), "=r"(r.w[3])
+      : "r"(d0), "r"(d1), "r"(d2), "r"(d3), "r"(m0), "r"(m1), "r"(m2), "r"(m3));
+  return r;
+}
+
+// ------------------------------------------------------------------ ArithFast
+
+// p = a * b, full 256-bit product, operand scanning with two carry chains per
+// row (low halves, then high halves of the 32x32 products).
+__device__ __forceinline__ void mul_128x128(const U128& a, const U128& b, uint32_t p[8]) {
+  asm("mul.lo.u32     %0, %8, %12;\n\t"
+      "mul.hi.u32     %1, %8, %12;\n\t"
+      "mad.lo.cc.u32  %1, %9, %12, %1;\n\t"
+      "madc.hi.u32    %2, %9, %12, 0;\n\t"
+      "mad.lo.cc.u32  %2, %10, %12, %2;\n\t"
+      "madc.hi.u32    %3, %10, %12, 0;\n\t"
+      "mad.lo.cc.u32  %3, %11, %12, %3;\n\t"
+      "madc.hi.u32    %4, %11, %12, 0;\n\t"
+      // row 1
+      "mad.lo.cc.u32  %1, %8, %13, %1;\n\t"
+      "madc.lo.cc.u32 %2, %9, %13, %2;\n\t"
+      "madc.lo.cc.u32 %3, %10, %13, %3;\n\t"
+      "madc.lo.cc.u32 %4, %11, %13, %4;\n\t"
+      "addc.u32       %5, 0, 0;\n\t"
+      "mad.hi.cc.u32  %2, %8, %13, %2;\n\t"
+      "madc.hi.cc.u32 %3, %9, %13, %3;\n\t"
+      "madc.hi.cc.u32 %4, %10, %13, %4;\n\t"
+      "madc.hi.u32    %5, %11, %13, %5;\n\t"
+      // row 2
+      "mad.lo.cc.u32  %2, %8, %14, %2;\n\t"
+      "madc.lo.cc.u32 %3, %9, %14, %3;\n\t"
+      "madc.lo.cc.u32 %4, %10, %14, %4;\n\t"
+      "madc.lo.cc.u32 %5, %11, %14, %5;\n\t"
+      "addc.u32       %6, 0, 0;\n\t"
+      "mad.hi.cc.u32  %3, %8, %14, %3;\n\t"
+      "madc.hi.cc.u32 %4, %9, %14, %4;\n\t"
+      "madc.hi.cc.u32 %5, %10, %14, %5;\n\t"
+      "madc.hi.u32    %6, %11, %14, %6;\n\t"
+      // row 3
+      "mad.lo.cc.u32  %3, %8, %15, %3;\n\t"
+      "madc.lo.cc.u32 %4, %9, %15, %4;\n\t"
+      "madc.lo.cc.u32 %5, %10, %15, %5;\n\t"
+      "madc.lo.cc.u32 %6, %11, %15, %6;\n\t"
+      "addc.u32       %7, 0, 0;\n\t"
+      "mad.hi.cc.u32  %4, %8, %15, %4;\n\t"
+      "madc.hi.cc.u32 %5, %9, %15, %5;\n\t"
+      "madc.hi.cc.u32 %6, %10, %15, %6;\n\t"
+      "madc.hi.u32    %7, %11, %15, %7;\n\t"
+      : "=&r"(p[0]), "=&r"(p[1]), "=&r"(p[2]), "=&r"(p[3]), "=&r"(p[4]), "=&r"(p[5]),
+        "=&r"(p[6]), "=&r"(p[7])
+      : "r"(a.w[0]), "r"(a.w[1]), "r"(a.w[2]), "r"(a.w[3]), "r"(b.w[0]), "r"(b.w[1]),
+        "r"(b.w[2]), "r"(b.w[3]));
+}
+
+// r = P mod q for q = 2^124 - k, P < 2^248, k < 2^14.
+//   P = H*2^124 + L      ->  t = L + H*k            (< 2^139)
+//   t = H2*2^124 + L2    ->  u = L2 + H2*k          (< 2^124 + 2^29 < 2q)
+//   r = u >= q ? u - q : u, tested as bit 124 of u + k.
+__device__ __forceinline__ U128 reduce_pm124(const uint32_t p[8], uint32_t k) {
+  const uint32_t h0 = __funnelshift_r(p[3], p[4], 28);
+  const uint32_t h1 = __funnelshift_r(p[4], p[5], 28);
+  const uint32_t h2 = __funnelshift_r(p[5], p[6], 28);
+  const uint32_t h3 = __funnelshift_r(p[6], p[7], 28);
+  const uint32_t l3 = p[3] & 0x0FFFFFFFu;
+  uint32_t t0, t1, t2, t3, t4;
+  asm("mad.lo.cc.u32  %0, %5, %9, %10;\n\t"
+      "madc.lo.cc.u32 %1, %6, %9, %11;\n\t"
+      "madc.lo.cc.u32 %2, %7, %9, %12;\n\t"
+      "madc.lo.cc.u32 %3, %8, %9, %13;\n\t"
+      "addc.u32       %4, 0, 0;\n\t"
+      "mad.hi.cc.u32  %1, %5, %9, %1;\n\t"
+      "madc.hi.cc.u32 %2, %6, %9, %2;\n\t"
+      "madc.hi.cc.u32 %3, %7, %9, %3;\n\t"
+      "madc.hi.u32    %4, %8, %9, %4;\n\t"
+      : "=&r"(t0), "=&r"(t1), "=&r"(t2), "=&r"(t3), "=&r"(t4)
+      : "r"(h0), "r"(h1), "r"(h2), "r"(h3), "r"(k), "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(l3));
+  const uint32_t u = __funnelshift_r(t3, t4, 28) * k;
+  uint32_t r0, r1, r2, r3, s0, s1, s2, s3;
+  asm("add.cc.u32  %0, %8, %12;\n\t"
+      "addc.cc.u32 %1, %9, 0;\n\t"
+      "addc.cc.u32 %2, %10, 0;\n\t"
+      "addc.u32    %3, %11, 0;\n\t"
+      "add.cc.u32  %4, %0, %13;\n\t"
+      "addc.cc.u32 %5, %1, 0;\n\t"
+      "addc.cc.u32 %6, %2, 0;\n\t"
+      "addc.u32    %7, %3, 0;\n\t"
+      : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3), "=&r"(s0), "=&r"(s1), "=&r"(s2), "=&r"(s3)
+      : "r"(t0), "r"(t1), "r"(t2), "r"(t3 & 0x0FFFFFFFu), "r"(u), "r"(k));
+  const bool ge = (s3 >> 28) != 0u;
+  U128 r;
+  r.w[0] = ge ? s0 : r0;
+  r.w[1] = ge ? s1 : r1;
+  r.w[2] = ge ? s2 : r2;
+  r.w[3] = ge ? (s3 & 0x0FFFFFFFu) : r3;
+  return r;
+}
+
+struct ArithFast {
+  static constexpr bool kFast = true;
+  __device__ __forceinline__ static U128 mul(const U128& a, const U128& b, const ModParams& m) {
+    uint32_t p[8];
+    mul_128x128(a, b, p);
+    return reduce_pm124(p, m.k);
+  }
+};
+
+// ------------------------------------------------------------------- ArithRef
+
+struct W128 {
+  uint64_t hi, lo;
+};
+
+__device__ __forceinline__ W128 w_add(W128 a, W128 b) {  // mod 2^128
+  W128 r;
+  r.lo = a.lo + b.lo;
+  r.hi = a.hi + b.hi + (r.lo < a.lo ? 1ull : 0ull);
+  return r;
+}
+__device__ __forceinline__ W128 w_mul64(uint64_t a, uint64_t b) {
+  return W128{__umul64hi(a, b), a * b};
+}
+__device__ __forceinline__ W128 to_w(const U128& a) {
+  return W128{((uint64_t)a.w[3] << 32) | a.w[2], ((uint64_t)a.w[1] << 32) | a.w[0]};
+}
+__device__ __forceinline__ U128 from_w(W128 a) {
+  U128 r;
+  r.w[0] = (uint32_t)a.lo; r.w[1] = (uint32_t)(a.lo >> 32);
+  r.w[2] = (uint32_t)a.hi; r.w[3] = (uint32_t)(a.hi >> 32);
+  return r;
+}
+
+// Reference mulmod128 with MBITS = 124, word for word: the 128x128 product
+// keeps its middle sum to 128 bits (src/ntt_scalar.c:106-128), the high
+// product of the quotient estimate likewise (:151-171), the low product keeps
+// its cross terms to 64 bits (:130-149), and one conditional subtraction ends
+// it (:194-196).
+struct ArithRef {
+  static constexpr bool kFast = false;
+  __device__ __forceinline__ static U128 mul(const U128& ua, const U128& ub, const ModParams& m) {
+    const W128 a = to_w(ua), b = to_w(ub), q = to_w(m.q), mu = to_w(m.mu);
+    // product
+    W128 p00 = w_mul64(a.lo, b.lo), p01 = w_mul64(a.lo, b.hi);
+    W128 p10 = w_mul64(a.hi, b.lo), p11 = w_mul64(a.hi, b.hi);
+    W128 mid = w_add(w_add(p01, p10), W128{0, p00.hi});
+    W128 ph = w_add(p11, W128{0, mid.hi});
+    W128 pl = W128{mid.lo, p00.lo};
+    // quotient estimate from bits 122.. of the product
+    // t = (P >> 122) mod 2^128 = (ph << 6) | (pl >> 122)
+    W128 t = W128{(ph.hi << 6) | (ph.lo >> 58), (ph.lo << 6) | (pl.hi >> 58)};
+    uint64_t top = ph.hi >> 58;
+    W128 m01 = w_mul64(t.lo, mu.hi), m10 = w_mul64(t.hi, mu.lo), m11 = w_mul64(t.hi, mu.hi);
+    W128 mm = w_add(w_add(m01, m10), W128{0, __umul64hi(t.lo, mu.lo)});
+    W128 qm = w_add(w_add(m11, W128{0, mm.hi}), W128{0, top * mu.lo});
+    W128 qq = W128{qm.hi >> 1, (qm.lo >> 1) | (qm.hi << 63)};
+    // low product qq*q
+    W128 l00 = w_mul64(qq.lo, q.lo);
+    uint64_t cross = qq.lo * q.hi + qq.hi * q.lo + l00.hi;
+    W128 qql = W128{cross, l00.lo};
+    // r = pl - qql mod 2^128
+    W128 r;
+    r.lo = pl.lo - qql.lo;
+    r.hi = pl.hi - qql.hi - (pl.lo < qql.lo ? 1ull : 0ull);
+    const bool lt = (r.hi < q.hi) || (r.hi == q.hi && r.lo < q.lo);
+    if (!lt) {
+      uint64_t lo2 = r.lo - q.lo;
+      r.hi = r.hi - q.hi - (r.lo < q.lo ? 1ull : 0ull);
+      r.lo = lo2;
+    }
+    return from_w(r);
+  }
+};
+
+// One butterfly of the network: (x, y) <- (x + w*y, x - w*y) with the
+// reference's addmod / submod (src/ntt_scalar.c:586-588).
+template <class Arith>
+__device__ __forceinline__ void butterfly(U128& x, U128& y, const U128& w, const ModParams& m) {
+  const U128 p = Arith::mul(w, y, m);
+  const U128 s = addmod_ref(x, p, m.q);
+  y = submod_ref(x, p, m.q);
+  x = s;
+}
+
+}  // namespace bntt

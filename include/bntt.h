@@ -1,0 +1,216 @@
+/*
+ * bntt.h -- C ABI of libbntt, a B200 (sm_100a) implementation of benchNTT's
+ * 128-bit modular NTT and BLAS-style vector operations.
+ *
+ * Results are bit-identical to the reference scalar path
+ * (src/ntt_scalar.c, src/blas_scalar.c of benchNTT) on the same inputs.
+ *
+ * Conventions
+ *   - Every function returns an int status (bntt_status).  On failure
+ *     bntt_last_error() gives a message for the calling thread.  Nothing
+ *     calls exit() (the reference loader does, src/config.c:11-14).
+ *   - 128-bit scalars cross the ABI as bntt_u128 {hi, lo}.
+ *   - Element buffers hold 16-byte residues in one of two layouts:
+ *       BNTT_LAYOUT_HILO  u64 pairs, high word first: the layout of the
+ *                         reference's data files and SIMD entry points
+ *                         (src/config.c:29-30, src/ntt_avx512.c:386)
+ *       BNTT_LAYOUT_U128  native little-endian unsigned __int128: the
+ *                         reference scalar API's uint128_t arrays
+ *                         (src/ntt_scalar.c:582)
+ *   - "_dev" functions take device pointers and are asynchronous on the
+ *     context's stream; "_host" functions take host pointers and return when
+ *     the result is in host memory.  Device pointers must be 16-byte aligned.
+ *   - Inputs are residues in [0, q] as in the reference (its data are in
+ *     [0, q); intermediate values may equal q).  With the default arithmetic
+ *     the results equal the reference's for every such input; with
+ *     BNTT_ARITH_REFERENCE they equal it for any 128-bit input.
+ *   - A context is used by one host thread at a time.
+ */
+#ifndef BNTT_H
+#define BNTT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BNTT_VERSION_MAJOR 0
+#define BNTT_VERSION_MINOR 1
+
+typedef enum bntt_status {
+    BNTT_OK = 0,
+    BNTT_EINVAL = 1,     /* bad argument: null pointer, size, log2n, alignment, layout */
+    BNTT_ENOMEM = 2,     /* device or pinned-host allocation failed */
+    BNTT_EBUDGET = 3,    /* request does not fit the context's HBM budget */
+    BNTT_ECUDA = 4,      /* CUDA runtime error; text in bntt_last_error() */
+    BNTT_ETIMEOUT = 5,   /* a bounded device-side wait gave up */
+    BNTT_ENODEV = 6,     /* no usable CUDA device */
+    BNTT_EBUSY = 7       /* object is in use (e.g. server running) */
+} bntt_status;
+
+typedef struct bntt_u128 {
+    uint64_t hi;
+    uint64_t lo;
+} bntt_u128;
+
+/* Modulus and Barrett constant with the reference's MBITS = 124
+ * (src/ntt_scalar.c:28-29): mu = floor(2^251 / q). */
+typedef struct bntt_modulus {
+    bntt_u128 q;
+    bntt_u128 mu;
+} bntt_modulus;
+
+#define BNTT_LAYOUT_HILO 0
+#define BNTT_LAYOUT_U128 1
+
+/* Arithmetic selection.
+ * AUTO: a pseudo-Mersenne multiply when q = 2^124 - k (k < 2^14) and
+ *       mu = floor(2^251/q) -- both reference moduli -- for which the
+ *       reference's Barrett reduction provably returns a*b mod q exactly;
+ *       otherwise the replica below.
+ * REFERENCE: a word-for-word replica of mulmod128 (src/ntt_scalar.c:173-199),
+ *       identical to the reference for any 128-bit operands. */
+#define BNTT_ARITH_AUTO 0
+#define BNTT_ARITH_REFERENCE 1
+
+typedef struct bntt_ctx bntt_ctx;
+typedef struct bntt_plan bntt_plan;
+typedef struct bntt_batch bntt_batch;
+
+/* ------------------------------------------------------------------ basics */
+const char *bntt_version(void);
+const char *bntt_last_error(void);
+const char *bntt_status_string(int status);
+
+/* 1 if `m` takes the fast multiply under BNTT_ARITH_AUTO, else 0. */
+int bntt_modulus_is_fast(const bntt_modulus *m);
+
+/* The moduli the reference programs use: the NTT drivers' q = 2^124 - 719
+ * (src/ntt_scalar.c:632-633) and the BLAS drivers' q = 2^124 - 59
+ * (src/blas_scalar.c:23-30). */
+bntt_modulus bntt_modulus_ntt_reference(void);
+bntt_modulus bntt_modulus_blas_reference(void);
+
+/* Context: device, stream, allocator accounting and HBM budget.
+ * `stream` is a cudaStream_t to run on, or NULL for a new non-blocking one. */
+int bntt_ctx_create(bntt_ctx **ctx, int device, void *stream);
+int bntt_ctx_destroy(bntt_ctx *ctx);
+int bntt_ctx_synchronize(bntt_ctx *ctx);
+void *bntt_ctx_stream(bntt_ctx *ctx);
+int bntt_ctx_set_arith(bntt_ctx *ctx, int arith);
+/* Cap on device bytes the context may hold (0 = no cap). */
+int bntt_ctx_set_hbm_budget(bntt_ctx *ctx, size_t bytes);
+size_t bntt_ctx_hbm_in_use(bntt_ctx *ctx);
+int bntt_ctx_sm_count(bntt_ctx *ctx);
+
+/* Device buffers charged to the context's budget. */
+int bntt_dev_alloc(bntt_ctx *ctx, void **ptr, size_t bytes);
+int bntt_dev_free(bntt_ctx *ctx, void *ptr);
+int bntt_copy_h2d(bntt_ctx *ctx, void *dst_dev, const void *src_host, size_t bytes);
+int bntt_copy_d2h(bntt_ctx *ctx, void *dst_host, const void *src_dev, size_t bytes);
+
+/* Seeded uniform residues in [0, q) (counter-based SplitMix64; element i
+ * depends only on seed and offset + i).  Host and device fills agree. */
+int bntt_fill_uniform_host(void *buf, size_t count, uint64_t seed, uint64_t offset,
+                           const bntt_modulus *m, int layout);
+int bntt_fill_uniform_dev(bntt_ctx *ctx, void *buf_dev, size_t count, uint64_t seed,
+                          uint64_t offset, const bntt_modulus *m, int layout);
+
+/* -------------------------------------------------------------------- NTT */
+/* A plan holds one transform size, modulus and twiddle table, uploaded once
+ * and kept in HBM (what ntt_pre prepares per call in the SIMD drivers,
+ * src/ntt_avx512.c:386-460).  `twiddles` is a host array of 2^log2n
+ * elements; entry 0 is never read (src/ntt_scalar.c:586-622).
+ * 1 <= log2n <= 24. */
+int bntt_plan_create(bntt_ctx *ctx, bntt_plan **plan, unsigned log2n, const bntt_modulus *m,
+                     const void *twiddles, int layout);
+/* Same, with the table already in device memory (not copied; must outlive
+ * the plan). */
+int bntt_plan_create_dev(bntt_ctx *ctx, bntt_plan **plan, unsigned log2n,
+                         const bntt_modulus *m, const void *twiddles_dev, int layout);
+int bntt_plan_destroy(bntt_plan *plan);
+unsigned bntt_plan_log2n(const bntt_plan *plan);
+
+/* Forward transform of `batch` contiguous inputs (replaces ntt(),
+ * src/ntt_scalar.c:582).  y may equal x.  One launch for 2^log2n <= 1024,
+ * one launch per HBM pass above. */
+int bntt_ntt_forward_dev(bntt_plan *plan, void *y, const void *x, size_t batch);
+/* Host-pointer form: copies in, transforms, copies out (the reference's
+ * call shape; pipelined over chunks of the batch). */
+int bntt_ntt_forward_host(bntt_plan *plan, void *y, const void *x, size_t batch);
+
+/* ------------------------------------------------------- mixed-size batch */
+/* One transform of a mixed batch: x and y are device pointers (or host
+ * pointers for bntt_batch_run_host) to 2^log2n elements of plans[plan]. */
+typedef struct bntt_job {
+    const void *x;
+    void *y;
+    uint32_t plan;
+    uint32_t reserved;
+} bntt_job;
+
+/* A batch object runs many independent transforms of uneven sizes in one
+ * persistent work-queue kernel.  `plans` must all use the same modulus and
+ * layout and outlive the batch. */
+int bntt_batch_create(bntt_ctx *ctx, bntt_batch **batch, bntt_plan *const *plans,
+                      size_t nplans);
+int bntt_batch_destroy(bntt_batch *batch);
+/* Device pointers, asynchronous.  The schedule (work items, their order and
+ * the per-size kernel shapes) is rebuilt only when the job list changes; the
+ * launch is replayed from a CUDA graph. */
+int bntt_batch_run_dev(bntt_batch *batch, const bntt_job *jobs, size_t count);
+/* Host pointers: inputs copied in, batch run, outputs copied back. */
+int bntt_batch_run_host(bntt_batch *batch, const bntt_job *jobs, size_t count);
+/* The same jobs, each launched on its own (one launch per transform of at
+ * most 1024 points, one per HBM pass above): the per-call path the
+ * persistent kernel is compared with.  Device pointers, asynchronous. */
+int bntt_batch_run_percall_dev(bntt_batch *batch, const bntt_job *jobs, size_t count);
+/* Status of the last run: BNTT_OK, or BNTT_ETIMEOUT if a device-side wait
+ * gave up (synchronises the stream). */
+int bntt_batch_status(bntt_batch *batch);
+/* Kernel launches the last run issued (graph replays count their kernels). */
+size_t bntt_batch_last_launches(bntt_batch *batch);
+
+/* ------------------------------------------------------------------- BLAS */
+/* Element-wise mod-q operations over `len` elements (the reference fixes
+ * len = 1024, src/blas_scalar.c:580):
+ *   vvadd  c[i] = addmod(a[i], b[i])            src/blas_scalar.c:578
+ *   vvsub  c[i] = submod(a[i], b[i])            src/blas_scalar.c:586
+ *   vvmul  c[i] = mulmod(a[i], b[i])            src/blas_scalar.c:594
+ *   axpy   c[i] = addmod(a[i], mulmod(x, b[i])) src/blas_scalar.c:602
+ * c may alias a or b. */
+int bntt_vvadd_dev(bntt_ctx *ctx, void *c, const void *a, const void *b, size_t len,
+                   const bntt_modulus *m, int layout);
+int bntt_vvsub_dev(bntt_ctx *ctx, void *c, const void *a, const void *b, size_t len,
+                   const bntt_modulus *m, int layout);
+int bntt_vvmul_dev(bntt_ctx *ctx, void *c, const void *a, const void *b, size_t len,
+                   const bntt_modulus *m, int layout);
+int bntt_axpy_dev(bntt_ctx *ctx, void *c, const void *a, const void *b, bntt_u128 x, size_t len,
+                  const bntt_modulus *m, int layout);
+
+int bntt_vvadd_host(bntt_ctx *ctx, void *c, const void *a, const void *b, size_t len,
+                    const bntt_modulus *m, int layout);
+int bntt_vvsub_host(bntt_ctx *ctx, void *c, const void *a, const void *b, size_t len,
+                    const bntt_modulus *m, int layout);
+int bntt_vvmul_host(bntt_ctx *ctx, void *c, const void *a, const void *b, size_t len,
+                    const bntt_modulus *m, int layout);
+int bntt_axpy_host(bntt_ctx *ctx, void *c, const void *a, const void *b, bntt_u128 x,
+                   size_t len, const bntt_modulus *m, int layout);
+
+/* Kernel launches issued by this context since creation (all entry points). */
+uint64_t bntt_ctx_launch_count(bntt_ctx *ctx);
+
+/* ------------------------------------------------------------ diagnostics */
+/* Measured throughput of the 32-bit integer multiply-add pipe on this device
+ * (independent mad.lo.u32 chains on every SM), in operations per second: the
+ * roofline the NTT kernels are reported against.  No reference counterpart
+ * (the reference times CPU code only, src/ntt_scalar.c:670-683). */
+int bntt_probe_imad_peak(bntt_ctx *ctx, double *ops_per_second);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BNTT_H */

@@ -14,7 +14,8 @@
  *
  * Buffers are hi-first u64 pairs (src/config.c:29-30).  Batch calls split the
  * work over `threads` POSIX threads, each with private scratch; the reference
- * globals (SIMD constants one/negone/t) are read-only after ref_init().
+ * globals (SIMD constants one/negone/t) are read-only after ref_init().  Batch
+ * calls return the wall time of the work itself (after scratch allocation).
  */
 #include <stdint.h>
 #include <stdlib.h>
@@ -105,8 +106,28 @@ static void *xalloc(size_t bytes)
     return p;
 }
 
+#include <time.h>
+
 typedef void (*range_fn)(void *ctx, size_t begin, size_t end);
 struct par { range_fn fn; void *ctx; size_t n; int threads; int id; };
+
+/* Timing: every thread allocates its scratch, then waits at this barrier;
+ * the clock runs from the barrier to the last thread's end, as the reference
+ * drivers allocate before their timing loops (src/ntt_scalar.c:635-638). */
+static pthread_barrier_t g_barrier;
+static int g_barrier_on = 0;
+static double g_t0;
+static double now_s(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+static void start_gate(void)
+{
+    if (!g_barrier_on) return;
+    if (pthread_barrier_wait(&g_barrier) == PTHREAD_BARRIER_SERIAL_THREAD) g_t0 = now_s();
+}
 
 static void *par_body(void *arg)
 {
@@ -115,14 +136,20 @@ static void *par_body(void *arg)
     size_t b = per * (size_t)p->id, e = b + per;
     if (e > p->n) e = p->n;
     if (b < e) p->fn(p->ctx, b, e);
+    else start_gate();
     return NULL;
 }
 
-static void parallel_for(range_fn fn, void *ctx, size_t n, int threads)
+/* Runs fn over [0, n) on `threads` threads; returns the seconds from the
+ * start gate to the end of the last thread. */
+static double parallel_for(range_fn fn, void *ctx, size_t n, int threads)
 {
     ref_init();
-    if (threads <= 1 || n <= 1) { fn(ctx, 0, n); return; }
-    if ((size_t)threads > n) threads = (int)n;
+    if (threads < 1) threads = 1;
+    if ((size_t)threads > n) threads = n ? (int)n : 1;
+    pthread_barrier_init(&g_barrier, NULL, (unsigned)threads);
+    g_barrier_on = 1;
+    g_t0 = now_s();
     pthread_t *th = malloc(sizeof(pthread_t) * (size_t)threads);
     struct par *ps = malloc(sizeof(struct par) * (size_t)threads);
     for (int i = 0; i < threads; ++i) {
@@ -130,7 +157,11 @@ static void parallel_for(range_fn fn, void *ctx, size_t n, int threads)
         pthread_create(&th[i], NULL, par_body, &ps[i]);
     }
     for (int i = 0; i < threads; ++i) pthread_join(th[i], NULL);
+    double t = now_s() - g_t0;
+    g_barrier_on = 0;
+    pthread_barrier_destroy(&g_barrier);
     free(th); free(ps);
+    return t;
 }
 
 /* --------------------------------------------------------------- scalar KAT */
@@ -185,6 +216,7 @@ static void ntt_range(void *vctx, size_t b, size_t e)
     uint128_t *x = xalloc(n * 16), *y = xalloc(n * 16), *tw = xalloc(n * 16);
     uint128_t *as0 = xalloc(n * 16), *as1 = xalloc(n * 16);
     for (size_t i = 0; i < n; ++i) tw[i] = MK(c->T[2 * i], c->T[2 * i + 1]);
+    start_gate();
     for (size_t j = b; j < e; ++j) {
         const uint64_t *xs = c->X + 2 * n * j;
         uint64_t *ys = c->Y + 2 * n * j;
@@ -203,6 +235,7 @@ static void ntt_range(void *vctx, size_t b, size_t e)
     vec *ash = xalloc(sizeof(vec) * v), *asl = xalloc(sizeof(vec) * v);
     vec *th = xalloc(sizeof(vec) * v), *tl = xalloc(sizeof(vec) * v);
     vec mh, ml, muh, mul;
+    start_gate();
     for (size_t j = b; j < e; ++j) {
         uint64_t *xs = (uint64_t *)(c->X + 2 * n * j);
         uint64_t *ys = c->Y + 2 * n * j;
@@ -224,11 +257,11 @@ static void ntt_range(void *vctx, size_t b, size_t e)
 /* `batch` contiguous transforms of N = 2^REF_STAGES hi-first pairs sharing
  * table T; each transform is the reference's full per-call sequence
  * (scalar: ntt(); SIMD: ntt_pre + ntt + ntt_post). */
-void bntt_ref_ntt_batch(uint64_t *Y, const uint64_t *X, const uint64_t *T, size_t batch,
-                        uint64_t mh, uint64_t ml, uint64_t muh, uint64_t mul, int threads)
+double bntt_ref_ntt_batch(uint64_t *Y, const uint64_t *X, const uint64_t *T, size_t batch,
+                          uint64_t mh, uint64_t ml, uint64_t muh, uint64_t mul, int threads)
 {
     struct ntt_ctx c = {Y, X, T, MK(mh, ml), MK(muh, mul)};
-    parallel_for(ntt_range, &c, batch, threads);
+    return parallel_for(ntt_range, &c, batch, threads);
 }
 #endif /* REF_KIND_NTT */
 
@@ -244,6 +277,7 @@ static void blas_range(void *vctx, size_t b, size_t e)
     struct blas_ctx *c = vctx;
 #if defined(REF_IMPL_SCALAR)
     uint128_t *a = xalloc(1024 * 16), *bb = xalloc(1024 * 16), *cc = xalloc(1024 * 16);
+    start_gate();
     for (size_t k = b; k < e; ++k) {
         const uint64_t *as = c->A + 2048 * k, *bs = c->B + 2048 * k;
         uint64_t *cs = c->C + 2048 * k;
@@ -262,6 +296,7 @@ static void blas_range(void *vctx, size_t b, size_t e)
     vec muh = SET1(c->mu >> 64), mul = SET1((uint64_t)c->mu);
     vec xh = SET1(c->x >> 64), xl = SET1((uint64_t)c->x);
     vec *sa = xalloc(1024 * 16), *sb = xalloc(1024 * 16), *sc = xalloc(1024 * 16);
+    start_gate();
     for (size_t k = b; k < e; ++k) {
         /* the SIMD kernels index vec arrays, so operands must be 64-byte
          * aligned; unaligned chunks are staged through aligned scratch */
@@ -283,13 +318,12 @@ static void blas_range(void *vctx, size_t b, size_t e)
 /* op: 0 vvadd, 1 vvsub, 2 vvmul, 3 axpy (c = a + x*b).  len must be a
  * multiple of 1024, the reference's fixed vector length
  * (src/blas_scalar.c:580); each 1024-element chunk is one reference call. */
-int bntt_ref_blas(int op, uint64_t *C, const uint64_t *A, const uint64_t *B, uint64_t xh,
-                  uint64_t xl, size_t len, uint64_t mh, uint64_t ml, uint64_t muh, uint64_t mul,
-                  int threads)
+double bntt_ref_blas(int op, uint64_t *C, const uint64_t *A, const uint64_t *B, uint64_t xh,
+                     uint64_t xl, size_t len, uint64_t mh, uint64_t ml, uint64_t muh, uint64_t mul,
+                     int threads)
 {
-    if (len % 1024) return -1;
+    if (len % 1024) return -1.0;
     struct blas_ctx c = {op, C, A, B, MK(xh, xl), MK(mh, ml), MK(muh, mul)};
-    parallel_for(blas_range, &c, len / 1024, threads);
-    return 0;
+    return parallel_for(blas_range, &c, len / 1024, threads);
 }
 #endif /* REF_KIND_BLAS */

@@ -1,0 +1,202 @@
+"""GPU parity of the persistent mixed-size batch engine (bntt_batch_*).
+
+Every job of a batch must equal the reference transform of its input
+(bit-exact); the same job must give the same bytes alone and inside a mix;
+graph replays and schedule rebuilds must not change results.
+"""
+import ctypes
+import hashlib
+
+import numpy as np
+import pytest
+
+import benchntt_b200 as bn
+import common as C
+from benchntt_b200 import workloads as W
+from gpu_util import DevBuf
+
+pytestmark = pytest.mark.gpu
+GEN = np.load(f"{C.GOLDEN}/ref_gen.npz")
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = bn.Context(0)
+    yield c
+    c.close()
+
+
+class Setup:
+    """Plans for every size of a workload, packed device input/output."""
+
+    def __init__(self, ctx, batch: W.Batch, q=C.Q_NTT, mu=C.MU_NTT, seed=W.SEED_INPUT):
+        self.ctx, self.batch = ctx, batch
+        self.tables = {n: C.uniform_pairs(W.SEED_TWIDDLE_BASE + n, 1 << n, q) for n in batch.sizes}
+        self.plans = {n: bn.Plan(ctx, n, q, mu, self.tables[n]) for n in batch.sizes}
+        self.plan_ids = {n: i for i, n in enumerate(batch.sizes)}
+        self.x = C.uniform_pairs(seed, batch.total, q)
+        self.dx = DevBuf.from_array(ctx, self.x)
+        self.dy = DevBuf(ctx, batch.total * 16)
+        self.engine = bn.Batch(ctx, [self.plans[n] for n in batch.sizes])
+
+    def jobs(self, idx=None, inplace=False):
+        idx = range(self.batch.count) if idx is None else idx
+        xs = [self.dx.addr + 16 * int(self.batch.offsets[i]) for i in idx]
+        ys = xs if inplace else [self.dy.addr + 16 * int(self.batch.offsets[i]) for i in idx]
+        return bn.Batch.jobs(xs, ys, [self.plan_ids[int(self.batch.logns[i])] for i in idx])
+
+    def output(self):
+        return self.dy.to_array(self.batch.total)
+
+    def expected(self, threads=8):
+        b = self.batch
+        xs = [self.x[o:o + (1 << n)] for o, n in zip(b.offsets, b.logns)]
+        ts = [self.tables[int(n)] for n in b.logns]
+        return np.concatenate(C.oracle_ntt_jobs(xs, ts, [int(n) for n in b.logns], threads=threads))
+
+    def close(self):
+        self.engine.close()
+        for p in self.plans.values():
+            p.close()
+        self.dx.free()
+        self.dy.free()
+
+
+def test_mixed_small_sizes(ctx):
+    b = W.uneven_batch(seed=1, n_small=3000, small_lo=1, small_hi=10, large=())
+    s = Setup(ctx, b)
+    s.engine.run_dev(s.jobs())
+    assert s.engine.status() == bn.OK
+    assert s.engine.last_launches == 1
+    assert np.array_equal(s.output(), s.expected())
+    s.close()
+
+
+def test_mixed_with_large_transforms(ctx):
+    b = W.uneven_batch(seed=2, n_small=2000, large=((11, 3), (13, 2), (16, 3), (20, 1)))
+    s = Setup(ctx, b)
+    s.engine.run_dev(s.jobs())
+    assert s.engine.status() == bn.OK
+    assert np.array_equal(s.output(), s.expected())
+    s.close()
+
+
+@pytest.mark.parametrize("logn", [16, 20])
+def test_large_job_matches_reference_fixture(ctx, logn):
+    """A 2^16 / 2^20 job inside a mix equals the compiled reference's output
+    on the fixture inputs (SHA-256 in tests/golden/ref_gen.npz)."""
+    n = 1 << logn
+    x = C.uniform_pairs(1000 + logn, n, C.Q_NTT)
+    t = C.uniform_pairs(2000 + logn, n, C.Q_NTT)
+    small_t = C.uniform_pairs(5, 1024, C.Q_NTT)
+    p_big = bn.Plan(ctx, logn, C.Q_NTT, C.MU_NTT, t)
+    p_small = bn.Plan(ctx, 10, C.Q_NTT, C.MU_NTT, small_t)
+    eng = bn.Batch(ctx, [p_big, p_small])
+    dx = DevBuf.from_array(ctx, x)
+    dy = DevBuf(ctx, n * 16)
+    xs_small = C.uniform_pairs(6, 1024 * 300, C.Q_NTT)
+    dxs = DevBuf.from_array(ctx, xs_small)
+    dys = DevBuf(ctx, xs_small.nbytes)
+    jobs = bn.Batch.jobs([dx.addr] + [dxs.addr + 16384 * i for i in range(300)],
+                         [dy.addr] + [dys.addr + 16384 * i for i in range(300)], [0] + [1] * 300)
+    eng.run_dev(jobs)
+    assert eng.status() == bn.OK
+    y = dy.to_array()
+    assert hashlib.sha256(y.astype("<u8").tobytes()).hexdigest() == str(GEN[f"ntt_sha_{logn}"])
+    assert np.array_equal(dys.to_array(), C.oracle_ntt(xs_small, small_t, 10, threads=8, form=1))
+    for d in (dx, dy, dxs, dys):
+        d.free()
+    eng.close()
+    p_big.close()
+    p_small.close()
+
+
+def test_job_alone_equals_job_in_mix(ctx):
+    b = W.uneven_batch(seed=3, n_small=1500, large=((16, 2), (20, 1)))
+    s = Setup(ctx, b)
+    s.engine.run_dev(s.jobs())
+    mixed = s.output()
+    for i in [0, 7, int(np.argmax(b.logns)), b.count - 1]:
+        s.engine.run_dev(s.jobs([i]))
+        assert s.engine.status() == bn.OK
+        o, n = int(b.offsets[i]), 1 << int(b.logns[i])
+        assert np.array_equal(s.output()[o:o + n], mixed[o:o + n])
+    s.close()
+
+
+def test_graph_replay_and_rebuild(ctx):
+    b = W.uneven_batch(seed=4, n_small=800, large=((12, 2),))
+    s = Setup(ctx, b)
+    want = s.expected()
+    jobs = s.jobs()
+    for _ in range(3):           # replay of the cached schedule
+        s.dy.ctx.synchronize()
+        s.engine.run_dev(jobs)
+        assert np.array_equal(s.output(), want)
+    sub = s.jobs(list(range(0, b.count, 3)))  # a different list rebuilds
+    s.engine.run_dev(sub)
+    assert s.engine.status() == bn.OK
+    s.engine.run_dev(jobs)
+    assert np.array_equal(s.output(), want)
+    s.close()
+
+
+def test_in_place_jobs(ctx):
+    b = W.uneven_batch(seed=5, n_small=500, large=((14, 1),))
+    s = Setup(ctx, b)
+    want = s.expected()
+    s.engine.run_dev(s.jobs(inplace=True))
+    assert s.engine.status() == bn.OK
+    assert np.array_equal(s.dx.to_array(b.total), want)
+    s.close()
+
+
+def test_run_host(ctx):
+    b = W.uneven_batch(seed=6, n_small=600, large=((16, 1),))
+    s = Setup(ctx, b)
+    y = np.zeros_like(s.x)
+    xs = [s.x.ctypes.data + 16 * int(o) for o in b.offsets]
+    ys = [y.ctypes.data + 16 * int(o) for o in b.offsets]
+    jobs = bn.Batch.jobs(xs, ys, [s.plan_ids[int(n)] for n in b.logns])
+    s.engine.run_host(jobs)
+    assert np.array_equal(y, s.expected())
+    s.close()
+
+
+def test_reference_arith_batch():
+    c = bn.Context(0, arith=bn.ARITH_REFERENCE)
+    b = W.uneven_batch(seed=7, n_small=400, large=((12, 1),))
+    s = Setup(c, b)
+    s.engine.run_dev(s.jobs())
+    assert np.array_equal(s.output(), s.expected())
+    s.close()
+    c.close()
+
+
+def test_invalid_jobs(ctx):
+    b = W.uneven_batch(seed=8, n_small=10, large=())
+    s = Setup(ctx, b)
+    jobs = s.jobs()
+    jobs[3].plan = 99
+    with pytest.raises(bn.BnttError) as e:
+        s.engine.run_dev(jobs)
+    assert e.value.status == bn.EINVAL
+    jobs = s.jobs()
+    jobs[2].x = s.dx.addr + 8
+    with pytest.raises(bn.BnttError):
+        s.engine.run_dev(jobs)
+    s.engine.run_dev(s.jobs())  # valid again
+    assert s.engine.status() == bn.OK
+    s.close()
+
+
+def test_full_uneven_batch_matches_oracle(ctx):
+    """The benchmark configuration: 100,000 transforms (N log-uniform over
+    2^4..2^10) + 64 x 2^16 + 4 x 2^20, one persistent launch, every job
+    bit-exact."""
+    b = W.uneven_batch()
+    s = Setup(ctx, b)
+    s.engine.run_dev(s.jobs())
+    assert s.engine.status() == bn.OK
+    assert np.array_equal(s.output(), s.expected(threads=16))
+    s.close()
