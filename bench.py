@@ -31,7 +31,6 @@ import os
 import statistics
 import subprocess
 import sys
-import tempfile
 import time
 
 import numpy as np
@@ -53,8 +52,8 @@ HBM_BYTES_PER_ELEM_BLAS = 48  # two 16-byte reads and one write
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0,
                     help="fraction of the uneven batch (profiling captures of a smaller case)")
@@ -100,56 +99,56 @@ class Dist:
 
 # ------------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi samples every 200 ms while the timed region runs."""
+    """SM clock, power and clock-event reasons polled through NVML (read only)
+    every ~5 ms while the timed region runs."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, device: int):
         self.device = device
-        self.proc = None
-        self.path = None
+        self.samples = []
+        self.thread = None
+        self.stop_flag = False
+        self.err = None
+
+    def _poll(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[self.device]) if vis else self.device
+            h = nv.nvmlDeviceGetHandleByIndex(idx)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            while not self.stop_flag:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                     nv.nvmlDeviceGetPowerUsage(h) / 1000.0, int(get_reasons(h))))
+                time.sleep(0.005)
+            nv.nvmlShutdown()
+        except Exception as e:  # NVML missing: report, do not fail the benchmark
+            self.err = repr(e)
 
     def start(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.device)],
-                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
-        time.sleep(0.25)
+        import threading
+        self.thread = threading.Thread(target=self._poll, daemon=True)
+        self.thread.start()
+        time.sleep(0.05)
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        time.sleep(0.25)
-        self.proc.terminate()
-        self.proc.wait()
-        rows = []
-        for line in open(self.path):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[4:]))
-            except ValueError:
-                continue
-        os.unlink(self.path)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        max_mhz = max(r[1] for r in rows)
-        peak_p = max(r[2] for r in rows)
-        loaded = [r for r in rows if r[2] >= 0.5 * peak_p] or rows
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in loaded for i, v in enumerate(r[3][1:5])
-                          if v.lower() == "active"})
-        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max_mhz,
-                "reasons": reasons, "samples": len(rows), "samples_under_load": len(loaded),
-                "power_w_max": peak_p}
+        self.stop_flag = True
+        if self.thread:
+            self.thread.join()
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "error": self.err}
+        peak_p = max(p for _, p, _ in self.samples)
+        loaded = [s for s in self.samples if s[1] >= 0.6 * peak_p] or self.samples
+        reasons = sorted({name for _, _, r in loaded for bit, name in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(c for c, _, _ in loaded), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples),
+                "samples_under_load": len(loaded), "power_w_max": peak_p, "source": "NVML"}
 
 
 # ---------------------------------------------------------------- CPU side
