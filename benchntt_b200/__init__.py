@@ -103,6 +103,7 @@ _SIGS = [
     ("bntt_batch_run_dev", _I, [_P, ctypes.POINTER(JobC), _S]),
     ("bntt_batch_run_host", _I, [_P, ctypes.POINTER(JobC), _S]),
     ("bntt_batch_run_percall_dev", _I, [_P, ctypes.POINTER(JobC), _S]),
+    ("bntt_batch_run_dev_noalloc", _I, [_P, ctypes.POINTER(JobC), _S]),
     ("bntt_batch_status", _I, [_P]),
     ("bntt_batch_last_launches", _S, [_P]),
     ("bntt_probe_imad_peak", _I, [_P, ctypes.POINTER(ctypes.c_double)]),
@@ -277,6 +278,10 @@ class Batch:
         arr = (ctypes.c_void_p * len(plans))(*[p.handle.value for p in plans])
         self._h = ctypes.c_void_p()
         check(lib().bntt_batch_create(ctx.handle, ctypes.byref(self._h), arr, len(plans)))
+
+    @property
+    def handle(self):
+        return self._h
 
     @staticmethod
     def jobs(xs: list[int], ys: list[int], plan_ids: list[int]):

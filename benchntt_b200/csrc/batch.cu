@@ -449,3 +449,93 @@ extern "C" int bntt_batch_run_percall_dev(bntt_batch* b, const bntt_job* jobs, s
   b->last_launches = (size_t)(b->ctx->launches - before);
   return BNTT_OK;
 }
+
+// ------------------------------------------------ run without allocating
+// Some callers cannot allocate device memory when they submit work: their
+// device memory is already reserved by another allocator (a framework's
+// caching pool that holds nearly all of HBM), or they sit on a latency
+// critical path where cudaMalloc / cudaFree would stall the device, or they
+// must not meet an out-of-memory error after initialisation.  For them the
+// batch run below keeps its scratch -- the work items, job descriptors, size
+// order and control words the persistent kernel reads and updates -- in one
+// fixed array compiled into the library instead of buffers from cudaMalloc.
+namespace bntt {
+
+constexpr size_t kNoAllocScratchBytes = 4u << 20;  // 4 MiB on every GPU that loads the library
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+static size_t round256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+}  // namespace bntt
+
+extern "C" int bntt_batch_run_dev_noalloc(bntt_batch* b, const bntt_job* jobs, size_t count) {
+  BNTT_REQUIRE(b && (jobs || count == 0), "NULL argument");
+  bntt_ctx* c = b->ctx;
+  if (int rc = ctx_use_device(c)) return rc;
+  BNTT_REQUIRE(c->device < kNoAllocMaxDevices, "device %d beyond the supported range", c->device);
+  if (count == 0) return BNTT_OK;
+  // Once per device, with that device current: the device address of the
+  // array (its name is only a host-side stand-in in host code).
+  void* base = nullptr;
+  {
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_base[c->device]) {
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(no-alloc scratch)");
+      g_noalloc_base[c->device] = p;
+    }
+    base = g_noalloc_base[c->device];
+  }
+  Schedule sc;  // host-side vectors only
+  if (int rc = build_schedule(b, sc, jobs, count)) return rc;
+  const size_t cb = (kCtlHeader + sc.nslots * kMaxPasses) * 4, pb = sc.pass_tiles.size() * 4,
+               ib = sc.items.size() * sizeof(WorkItem), ob = sc.order.size() * 4,
+               jb = sc.djobs.size() * sizeof(DevJob);
+  const size_t o_ctl = 0, o_pt = round256(o_ctl + cb), o_it = round256(o_pt + pb),
+               o_or = round256(o_it + ib), o_jb = round256(o_or + ob), need = round256(o_jb + jb);
+  if (need > kNoAllocScratchBytes)
+    return set_error(BNTT_EINVAL,
+                     "this job list needs %zu bytes of scratch; the no-allocation entry point "
+                     "holds at most %zu (about 70,000 transforms; split the list)",
+                     need, kNoAllocScratchBytes);
+  char* s = static_cast<char*>(base);
+  cudaStream_t st = c->stream;
+  // the array keeps the previous call's contents: the control words (queue
+  // head, error word, pass counters) must start at zero
+  BNTT_CK(cudaMemsetAsync(s + o_ctl, 0, cb, st));
+  if (pb) BNTT_CK(cudaMemcpyAsync(s + o_pt, sc.pass_tiles.data(), pb, cudaMemcpyHostToDevice, st));
+  if (ib) BNTT_CK(cudaMemcpyAsync(s + o_it, sc.items.data(), ib, cudaMemcpyHostToDevice, st));
+  if (ob) BNTT_CK(cudaMemcpyAsync(s + o_or, sc.order.data(), ob, cudaMemcpyHostToDevice, st));
+  if (jb) BNTT_CK(cudaMemcpyAsync(s + o_jb, sc.djobs.data(), jb, cudaMemcpyHostToDevice, st));
+  if (sc.items.empty()) return BNTT_OK;
+  const void* fn = batch_kernel(b->fast);
+  size_t smem = 0;
+  bool used[kNumShapes] = {};
+  for (const WorkItem& w : sc.items) used[w.shape] = true;
+  for (int k = 0; k < kNumShapes; ++k)
+    if (used[k]) smem = std::max(smem, shape_smem(k));
+  BNTT_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1)));
+  int bps = 0;
+  BNTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, kBatchThreads, smem));
+  if (bps < 1) return set_error(BNTT_ECUDA, "batch kernel does not fit on an SM (smem %zu)", smem);
+  const unsigned grid = (unsigned)std::min<size_t>((size_t)bps * c->sms, sc.items.size());
+  BatchArgs ba;
+  ba.items = reinterpret_cast<const WorkItem*>(s + o_it);
+  ba.nitems = (uint32_t)sc.items.size();
+  ba.jobs = reinterpret_cast<const DevJob*>(s + o_jb);
+  ba.order = reinterpret_cast<const uint32_t*>(s + o_or);
+  ba.ctl = reinterpret_cast<uint32_t*>(s + o_ctl);
+  ba.pass_tiles = reinterpret_cast<const uint32_t*>(s + o_pt);
+  ModParams mp = b->mp;
+  int layout = b->layout;
+  void* args[] = {&ba, &mp, &layout};
+  BNTT_CK(cudaLaunchKernel(fn, dim3(grid), dim3(kBatchThreads), args, smem, st));
+  c->launches++;
+  b->last_launches = 1;
+  return BNTT_OK;
+}

@@ -167,6 +167,22 @@ int bntt_batch_run_host(bntt_batch *batch, const bntt_job *jobs, size_t count);
  * most 1024 points, one per HBM pass above): the per-call path the
  * persistent kernel is compared with.  Device pointers, asynchronous. */
 int bntt_batch_run_percall_dev(bntt_batch *batch, const bntt_job *jobs, size_t count);
+/* Same as bntt_batch_run_dev, but allocates no device memory: for callers
+ * that cannot call cudaMalloc when they submit work (device memory owned by
+ * another allocator's pool, latency-critical paths where an allocation would
+ * stall the device, services that must not hit out-of-memory after start-up).
+ * No counterpart in the reference, which runs on the CPU only.
+ * Its scratch (work items, job descriptors, control words) lives in one
+ * 4 MiB array inside the library, present on every GPU that loads it until
+ * the process exits; a job list whose schedule needs more (roughly 70,000
+ * transforms) is rejected with BNTT_EINVAL.  The first call on a device looks
+ * up that array's device address; make that first call before any stream
+ * capture.  Every call reuses the same array: the control words are cleared
+ * on each call, and calls whose work overlaps on the GPU (several streams,
+ * contexts or threads on one device) race -- serialise them.  Asynchronous on
+ * the context's stream; a device-side wait that gives up is not reported
+ * here (use bntt_batch_run_dev when that check is needed). */
+int bntt_batch_run_dev_noalloc(bntt_batch *batch, const bntt_job *jobs, size_t count);
 /* Status of the last run: BNTT_OK, or BNTT_ETIMEOUT if a device-side wait
  * gave up (synchronises the stream). */
 int bntt_batch_status(bntt_batch *batch);
