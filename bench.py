@@ -59,6 +59,9 @@ def parse():
                     help="fraction of the uneven batch (profiling captures of a smaller case)")
     ap.add_argument("--headline-only", action="store_true",
                     help="only the persistent-kernel step (for profiler launch lists)")
+    ap.add_argument("--only", choices=["uniform", "blas"], default=None,
+                    help="run one secondary benchmark alone (profiling captures)")
+    ap.add_argument("--logn", type=int, default=10, help="size for --only uniform")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     return ap.parse_args()
 
@@ -269,6 +272,22 @@ def profiles_traffic(name: str):
     return None
 
 
+def run_only(args, dist: Dist):
+    """One secondary benchmark on its own (for ncu captures of one kernel)."""
+    import torch
+
+    import benchntt_b200 as bn
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    ctx = bn.Context(dev, stream=stream.cuda_stream)
+    if args.only == "uniform":
+        res = uniform_bench(args, ctx, stream, ctx.imad_peak(), sizes=[args.logn])
+    else:
+        res = blas_bench(args, ctx, stream, measured_peaks())
+    return {"only": args.only, "result": res}, ctx
+
+
 def run_ours(args, dist: Dist):
     import torch
 
@@ -280,7 +299,6 @@ def run_ours(args, dist: Dist):
     stream = torch.cuda.Stream(device=dev)
     ctx = bn.Context(dev, stream=stream.cuda_stream)
     L = bn.lib()
-    out = {}
 
     # ---------------------------------------------------- headline workload
     batch = W.uneven_batch()
@@ -469,10 +487,10 @@ def blas_bench(args, ctx, stream, peaks) -> dict:
             else:
                 bn.check(fn(ctx.handle, c.data_ptr(), a.data_ptr(), b.data_ptr(), n,
                             ctypes.byref(mod), 0))
-        for _ in range(max(3, args.warmup)):
+        for _ in range(max(1, args.warmup) if args.only else max(3, args.warmup)):
             go()
         e0, e1 = cuda_events()
-        reps = max(5, args.steps)
+        reps = max(1, args.steps) if args.only else max(5, args.steps)
         e0.record(stream)
         for _ in range(reps):
             go()
@@ -485,7 +503,7 @@ def blas_bench(args, ctx, stream, peaks) -> dict:
     return res
 
 
-def uniform_bench(args, ctx, stream, imad_peak) -> dict:
+def uniform_bench(args, ctx, stream, imad_peak, sizes=range(4, 11)) -> dict:
     """65,536 transforms of one size, one launch (config: uniform batch)."""
     import torch
 
@@ -494,17 +512,17 @@ def uniform_bench(args, ctx, stream, imad_peak) -> dict:
     mod = bn.modulus(Q_NTT, MU_NTT)
     res = {}
     count = 65536
-    for logn in range(4, 11):
+    for logn in sizes:
         n = 1 << logn
         x = torch.empty((n * count, 2), dtype=torch.int64, device=ctx.device)
         y = torch.empty_like(x)
         bn.check(L.bntt_fill_uniform_dev(ctx.handle, x.data_ptr(), n * count, 7, 0,
                                          ctypes.byref(mod), 0))
         plan = bn.Plan(ctx, logn, Q_NTT, MU_NTT, bn.fill_uniform(2000 + logn, n, Q_NTT))
-        for _ in range(3):
+        for _ in range(max(1, min(3, args.warmup))):
             plan.forward(y, x, count)
         e0, e1 = cuda_events()
-        reps = max(5, args.steps // 2)
+        reps = max(1, args.steps // 2) if args.only else max(5, args.steps // 2)
         e0.record(stream)
         for _ in range(reps):
             plan.forward(y, x, count)
@@ -560,6 +578,12 @@ def main():
             res = run_reference(args, dist)
             if res is not None:
                 print(json.dumps(res), flush=True)
+            return
+        if args.only:
+            res, ctx = run_only(args, dist)
+            if dist.rank == 0:
+                print(json.dumps(res), flush=True)
+            ctx.close()
             return
         res, ctx = run_ours(args, dist)
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu and not args.headline_only:

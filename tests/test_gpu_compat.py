@@ -1,0 +1,56 @@
+"""C programs in the shape of the reference drivers, linked against libbntt
+through include/bntt_compat.h and include/bntt_compat_simd.h, on the
+reference's golden data written in its text format."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import benchntt_b200 as bn
+import common as C
+
+pytestmark = pytest.mark.gpu
+SRC = os.path.join(C.ROOT, "tests", "compat")
+LIBDIR = os.path.dirname(bn.LIB_PATH)
+
+
+@pytest.fixture(scope="module")
+def datadir(tmp_path_factory):
+    d = tmp_path_factory.mktemp("data")
+    gold = C.load_golden()
+    for key in gold.files:   # x_N, twd_N, ver_N, <op>_1024: one decimal u64 per line
+        np.savetxt(d / f"{key}.txt", gold[key].reshape(-1), fmt="%d")
+    return str(d)
+
+
+def build(tmp_path, src, extra=()):
+    exe = str(tmp_path / (os.path.basename(src) + "".join(extra).replace("-", "_") + ".bin"))
+    subprocess.run(["gcc", "-O2", "-std=gnu11", *extra, "-I", os.path.join(C.ROOT, "include"),
+                    os.path.join(SRC, src), "-L", LIBDIR, "-lbntt", f"-Wl,-rpath,{LIBDIR}",
+                    "-o", exe], check=True)
+    return exe
+
+
+@pytest.mark.parametrize("stages", [4, 7, 10])
+def test_scalar_ntt_driver(tmp_path, datadir, stages):
+    exe = build(tmp_path, "ntt_scalar_driver.c", (f"-Dstages={stages}",))
+    out = subprocess.run([exe, datadir], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.strip() == f"{1 << stages} fail: 0"
+
+
+@pytest.mark.parametrize("stages", [5, 10])
+def test_simd_ntt_driver(tmp_path, datadir, stages):
+    exe = build(tmp_path, "ntt_simd_driver.c", (f"-Dstages={stages}", "-mavx2"))
+    out = subprocess.run([exe, datadir], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.strip() == f"{1 << stages} fail: 0"
+
+
+def test_blas_driver(tmp_path, datadir):
+    exe = build(tmp_path, "blas_driver.c")
+    out = subprocess.run([exe, datadir], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.split() == ["vvadd", "fail:", "0", "vvsub", "fail:", "0", "vvmul", "fail:",
+                                  "0", "axpy", "fail:", "0"]
