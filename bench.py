@@ -300,6 +300,14 @@ def run_ours(args, dist: Dist):
     ctx = bn.Context(dev, stream=stream.cuda_stream)
     L = bn.lib()
 
+    # ------------------------------------------------------------ autotuner
+    import tempfile
+    tune_path = os.path.join(tempfile.mkdtemp(), "bntt.tune")
+    t_tune = time.perf_counter()
+    ctx.autotune(tune_path)
+    tune_s = time.perf_counter() - t_tune
+    tuned = [l.strip() for l in open(tune_path) if l.startswith(("sub ", "batch "))]
+
     # ---------------------------------------------------- headline workload
     batch = W.uneven_batch()
     if args.scale < 1.0:
@@ -381,6 +389,8 @@ def run_ours(args, dist: Dist):
         "roofline": roofline,
         "clocks": clk,
         "parity": "bit-exact vs the reference: tests/test_gpu_batch.py::test_full_uneven_batch_matches_oracle",
+        "autotune": {"seconds": tune_s, "choices": tuned,
+                     "format": "sub m map fast logr tpc minb | batch m logr tpc"},
     }
     if args.headline_only:
         return result, ctx
@@ -393,8 +403,10 @@ def run_ours(args, dist: Dist):
     result["blas"] = blas_bench(args, ctx, stream, peaks)
     # --------------------------------------------------------- uniform sizes
     result["uniform"] = uniform_bench(args, ctx, stream, imad_peak)
+    # --------------------------------------------------------------- serving
     engine.close()
     del x, y
+    result["serving"] = serving_bench(args, ctx)
     for p in plans.values():
         p.close()
     return result, ctx
@@ -535,6 +547,62 @@ def uniform_bench(args, ctx, stream, imad_peak, sizes=range(4, 11)) -> dict:
         plan.close()
         del x, y
     return res
+
+
+def serving_bench(args, ctx) -> dict:
+    """Poisson arrivals at 50k requests/s: 70% forward NTTs with N log-uniform
+    over 2^4..2^20, 30% vvmul / axpy with length log-uniform over 2^10..2^22,
+    device-resident operands, 32 GiB admission budget.  Continuous batching
+    versus the same requests served one call at a time."""
+    import torch
+
+    import benchntt_b200 as bn
+    from benchntt_b200 import workloads as W
+    L = bn.lib()
+    sizes = list(range(4, 21))
+    plans = [bn.Plan(ctx, n, Q_NTT, MU_NTT, bn.fill_uniform(W.SEED_TWIDDLE_BASE + n, 1 << n, Q_NTT))
+             for n in sizes]
+    mod, modb = bn.modulus(Q_NTT, MU_NTT), bn.modulus(Q_BLAS, MU_BLAS)
+    ntt_in = {}
+    for n in sizes:     # one resident input per size
+        t = torch.empty((1 << n, 2), dtype=torch.int64, device=ctx.device)
+        bn.check(L.bntt_fill_uniform_dev(ctx.handle, t.data_ptr(), 1 << n, 100 + n, 0, ctypes.byref(mod), 0))
+        ntt_in[n] = t
+    blas_in = {}
+    for l in range(10, 23):
+        a = torch.empty((1 << l, 2), dtype=torch.int64, device=ctx.device)
+        b = torch.empty_like(a)
+        bn.check(L.bntt_fill_uniform_dev(ctx.handle, a.data_ptr(), 1 << l, 200 + l, 0, ctypes.byref(modb), 0))
+        bn.check(L.bntt_fill_uniform_dev(ctx.handle, b.data_ptr(), 1 << l, 300 + l, 0, ctypes.byref(modb), 0))
+        blas_in[l] = (a, b)
+    count = 20_000
+    trace = W.serving_trace(rate=50_000.0, count=count)
+    reqs = (bn.RequestC * count)()
+    for i, r in enumerate(trace):
+        q = reqs[i]
+        q.t_arrive, q.tag = r.t_arrive, i
+        if r.kind == "ntt":
+            q.kind, q.plan, q.x = bn.REQ_NTT, sizes.index(r.log2), ntt_in[r.log2].data_ptr()
+        else:
+            a, b = blas_in[r.log2]
+            q.kind = bn.REQ_VVMUL if r.kind == "vvmul" else bn.REQ_AXPY
+            q.len, q.x, q.b, q.scalar = 1 << r.log2, a.data_ptr(), b.data_ptr(), bn.U128.of(AXPY_X)
+    out = {"requests": count, "rate_req_s": 50_000, "mix": "70% NTT 2^4..2^20, 30% vvmul/axpy 2^10..2^22",
+           "hbm_budget_bytes": 32 << 30}
+    srv = bn.Server(ctx, plans, Q_BLAS, MU_BLAS, hbm_budget=32 << 30, slots=4, max_batch=4096)
+    warm = (bn.RequestC * 2000)(*reqs[:2000])   # warm-up on the first 2,000 arrivals
+    for mode, serial in (("continuous_batching", False), ("one_call_at_a_time", True)):
+        srv.replay(warm, serial=serial)
+        lat, wall = srv.replay(reqs, serial=serial)
+        out[mode] = {"throughput_req_s": count / wall, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                     "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                     "mean_ms": float(lat.mean() * 1e3), "wall_s": wall}
+    out["stats"] = srv.stats()
+    out["p99_speedup"] = out["one_call_at_a_time"]["p99_ms"] / out["continuous_batching"]["p99_ms"]
+    srv.close()
+    for p in plans:
+        p.close()
+    return out
 
 
 # ---------------------------------------------------------- reference arm

@@ -64,6 +64,31 @@ class JobC(ctypes.Structure):
                 ("reserved", ctypes.c_uint32)]
 
 
+class ServerConfigC(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_size_t), ("slots", ctypes.c_uint32),
+                ("max_batch", ctypes.c_uint32)]
+
+
+class RequestC(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint32), ("plan", ctypes.c_uint32), ("len", ctypes.c_uint64),
+                ("x", ctypes.c_void_p), ("b", ctypes.c_void_p), ("scalar", U128),
+                ("tag", ctypes.c_uint64), ("t_arrive", ctypes.c_double)]
+
+
+class CompletionC(ctypes.Structure):
+    _fields_ = [("tag", ctypes.c_uint64), ("y", ctypes.c_void_p), ("bytes", ctypes.c_size_t),
+                ("t_arrive", ctypes.c_double), ("t_admit", ctypes.c_double),
+                ("t_done", ctypes.c_double), ("status", ctypes.c_int)]
+
+
+class ServerStatsC(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64), ("admission_waits", ctypes.c_uint64),
+                ("peak_bytes", ctypes.c_size_t)]
+
+
+REQ_NTT, REQ_VVMUL, REQ_AXPY = 0, 1, 2
+
 _LIB = None
 
 # (name, restype, argtypes)
@@ -105,8 +130,23 @@ _SIGS = [
     ("bntt_batch_run_percall_dev", _I, [_P, ctypes.POINTER(JobC), _S]),
     ("bntt_batch_run_dev_noalloc", _I, [_P, ctypes.POINTER(JobC), _S]),
     ("bntt_batch_status", _I, [_P]),
+    ("bntt_batch_inject_wait_timeout", _I, [_P, ctypes.c_uint32]),
     ("bntt_batch_last_launches", _S, [_P]),
     ("bntt_probe_imad_peak", _I, [_P, ctypes.POINTER(ctypes.c_double)]),
+    ("bntt_server_create", _I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _S, _PM,
+                                ctypes.POINTER(ServerConfigC)]),
+    ("bntt_server_destroy", _I, [_P]),
+    ("bntt_server_clock", ctypes.c_double, [_P]),
+    ("bntt_server_submit", _I, [_P, ctypes.POINTER(RequestC)]),
+    ("bntt_server_poll", _I, [_P, ctypes.POINTER(CompletionC), _S, ctypes.POINTER(_S)]),
+    ("bntt_server_release", _I, [_P, _P]),
+    ("bntt_server_drain", _I, [_P]),
+    ("bntt_server_get_stats", _I, [_P, ctypes.POINTER(ServerStatsC)]),
+    ("bntt_server_replay", _I, [_P, ctypes.POINTER(RequestC), _S, _I,
+                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    ("bntt_autotune", _I, [_P, ctypes.c_char_p]),
+    ("bntt_autotune_load", _I, [_P, ctypes.c_char_p]),
+    ("bntt_autotune_reset", _I, []),
 ] + [(f"bntt_{op}_{kind}", _I, [_P, _P, _P, _P, _S, _PM, _I])
      for op in ("vvadd", "vvsub", "vvmul") for kind in ("dev", "host")] + [
     (f"bntt_axpy_{kind}", _I, [_P, _P, _P, _P, U128, _S, _PM, _I]) for kind in ("dev", "host")]
@@ -207,6 +247,14 @@ class Context:
     @property
     def launches(self) -> int:
         return lib().bntt_ctx_launch_count(self._h)
+
+    def autotune(self, path: str | None = None) -> None:
+        """Times the compiled kernel shapes on this device and makes the
+        fastest the defaults for plans / batches created afterwards."""
+        check(lib().bntt_autotune(self._h, path.encode() if path else None))
+
+    def autotune_load(self, path: str) -> None:
+        check(lib().bntt_autotune_load(self._h, path.encode()))
 
     def imad_peak(self) -> float:
         """Measured 32-bit IMAD operations per second of this device."""
@@ -310,6 +358,67 @@ class Batch:
     def close(self) -> None:
         if self._h:
             lib().bntt_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The serving loop (bntt_server_*): continuous batching of NTT / vvmul /
+    axpy requests on device-resident operands, admitted under an HBM budget."""
+
+    def __init__(self, ctx: Context, plans: list[Plan], blas_q: int, blas_mu: int,
+                 hbm_budget: int = 0, slots: int = 0, max_batch: int = 0):
+        self.ctx, self.plans = ctx, plans
+        self._blas = modulus(blas_q, blas_mu)
+        cfg = ServerConfigC(hbm_budget, slots, max_batch)
+        arr = (ctypes.c_void_p * len(plans))(*[p.handle.value for p in plans])
+        self._h = ctypes.c_void_p()
+        check(lib().bntt_server_create(ctx.handle, ctypes.byref(self._h), arr, len(plans),
+                                       ctypes.byref(self._blas), ctypes.byref(cfg)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def clock(self) -> float:
+        return lib().bntt_server_clock(self._h)
+
+    def submit(self, req: RequestC) -> None:
+        check(lib().bntt_server_submit(self._h, ctypes.byref(req)))
+
+    def poll(self, cap: int = 1024) -> list:
+        out = (CompletionC * cap)()
+        n = ctypes.c_size_t()
+        check(lib().bntt_server_poll(self._h, out, cap, ctypes.byref(n)))
+        return [out[i] for i in range(n.value)]
+
+    def release(self, y: int) -> None:
+        check(lib().bntt_server_release(self._h, y))
+
+    def drain(self) -> None:
+        check(lib().bntt_server_drain(self._h))
+
+    def stats(self) -> dict:
+        st = ServerStatsC()
+        check(lib().bntt_server_get_stats(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in ServerStatsC._fields_}
+
+    def replay(self, reqs, serial: bool = False):
+        """Latencies (s) of every request and the wall time of the replay."""
+        n = len(reqs)
+        lat = (ctypes.c_double * n)()
+        wall = ctypes.c_double()
+        check(lib().bntt_server_replay(self._h, reqs, n, 1 if serial else 0, lat, ctypes.byref(wall)))
+        return np.frombuffer(lat, dtype=np.float64).copy(), wall.value
+
+    def close(self) -> None:
+        if self._h:
+            lib().bntt_server_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

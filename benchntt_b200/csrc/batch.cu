@@ -4,14 +4,14 @@
 #include <algorithm>
 #include <cstring>
 
-#include "batch_dev.cuh"
+#include "batch_host.h"
 
 namespace bntt {
 
 const void* batch_kernel_fast();
 const void* batch_kernel_ref();
 
-static size_t shape_smem(int s) {
+size_t shape_smem(int s) {
   const BatchShape& b = kShapes[s];
   const int npass = (b.m + b.logr - 1) / b.logr;
   return npass > 1 ? (size_t)b.tpc * ((size_t)1 << b.m) * 16 : 0;
@@ -25,63 +25,13 @@ int batch_shape_for(int m, int map, int logr_pref) {
   return -1;
 }
 
-// Shape choice per size: small tiles, interleaved passes, contiguous passes.
-struct ShapeChoice {
-  int small[11];
-  int pass_il[11];
-  int pass_contig[11];
-};
-
-// One job list turned into work items, with its device copies and graph.
-struct Schedule {
-  std::vector<DevJob> djobs;
-  std::vector<uint32_t> order;
-  std::vector<WorkItem> items;
-  std::vector<uint32_t> pass_tiles;
-  size_t nslots = 0;
-  void* d_jobs = nullptr;
-  size_t d_jobs_cap = 0;
-  void* d_order = nullptr;
-  size_t d_order_cap = 0;
-  void* d_items = nullptr;
-  size_t d_items_cap = 0;
-  void* d_ctl = nullptr;
-  size_t d_ctl_cap = 0;
-  void* d_pass_tiles = nullptr;
-  size_t d_pass_tiles_cap = 0;
-  cudaGraphExec_t exec = nullptr;
-  cudaStream_t exec_stream = nullptr;  // stream the graph was captured on
-  int grid = 0;
-  size_t smem = 0;
-};
-
 }  // namespace bntt
 
 using namespace bntt;
 
-struct bntt_batch {
-  bntt_ctx* ctx = nullptr;
-  std::vector<bntt_plan*> plans;
-  ModParams mp{};
-  bool fast = false;
-  int layout = 0;
-  ShapeChoice shapes{};
-  // device-pointer runs
-  std::vector<bntt_job> last_jobs;
-  Schedule main;
-  // host-pointer runs: packed device region, job groups with own schedules
-  std::vector<bntt_job> host_last_jobs;
-  std::vector<Schedule> groups;
-  std::vector<size_t> group_first;   // first job of each group (+ end)
-  std::vector<size_t> dev_off;       // byte offset of each job in the region
-  void* region = nullptr;
-  size_t region_cap = 0;
-  size_t last_launches = 0;
-};
-
 namespace bntt {
 
-static int grow(bntt_ctx* c, void** p, size_t* cap, size_t bytes) {
+int grow(bntt_ctx* c, void** p, size_t* cap, size_t bytes) {
   if (*cap >= bytes && *p) return BNTT_OK;
   if (*p) ctx_free(c, *p);
   *p = nullptr;
@@ -92,7 +42,7 @@ static int grow(bntt_ctx* c, void** p, size_t* cap, size_t bytes) {
   return BNTT_OK;
 }
 
-static void free_schedule(bntt_ctx* c, Schedule& s) {
+void free_schedule(bntt_ctx* c, Schedule& s) {
   if (s.exec) cudaGraphExecDestroy(s.exec);
   s.exec = nullptr;
   for (void** p : {&s.d_jobs, &s.d_order, &s.d_items, &s.d_ctl, &s.d_pass_tiles}) {
@@ -102,9 +52,9 @@ static void free_schedule(bntt_ctx* c, Schedule& s) {
   s.d_jobs_cap = s.d_order_cap = s.d_items_cap = s.d_ctl_cap = s.d_pass_tiles_cap = 0;
 }
 
-static const void* batch_kernel(bool fast) { return fast ? batch_kernel_fast() : batch_kernel_ref(); }
+const void* batch_kernel(bool fast) { return fast ? batch_kernel_fast() : batch_kernel_ref(); }
 
-static int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count) {
+int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count) {
   sc.djobs.resize(count);
   sc.order.clear();
   sc.items.clear();
@@ -200,7 +150,12 @@ static int upload_and_capture(bntt_batch* b, Schedule& sc, cudaStream_t stream) 
   if (jb) BNTT_CK(cudaMemcpyAsync(sc.d_jobs, sc.djobs.data(), jb, cudaMemcpyHostToDevice, stream));
   if (ob) BNTT_CK(cudaMemcpyAsync(sc.d_order, sc.order.data(), ob, cudaMemcpyHostToDevice, stream));
   if (ib) BNTT_CK(cudaMemcpyAsync(sc.d_items, sc.items.data(), ib, cudaMemcpyHostToDevice, stream));
-  if (pb) BNTT_CK(cudaMemcpyAsync(sc.d_pass_tiles, sc.pass_tiles.data(), pb, cudaMemcpyHostToDevice, stream));
+  if (pb) {
+    std::vector<uint32_t> tiles = sc.pass_tiles;
+    if (b->inject_polls)  // injected fault: every wait needs one tile more than exists
+      for (uint32_t& t : tiles) t += 1;
+    BNTT_CK(cudaMemcpyAsync(sc.d_pass_tiles, tiles.data(), pb, cudaMemcpyHostToDevice, stream));
+  }
   BNTT_CK(cudaStreamSynchronize(stream));
   if (sc.exec) {
     cudaGraphExecDestroy(sc.exec);
@@ -226,6 +181,7 @@ static int upload_and_capture(bntt_batch* b, Schedule& sc, cudaStream_t stream) 
   ba.order = static_cast<const uint32_t*>(sc.d_order);
   ba.ctl = static_cast<uint32_t*>(sc.d_ctl);
   ba.pass_tiles = static_cast<const uint32_t*>(sc.d_pass_tiles);
+  ba.wait_polls = b->inject_polls ? b->inject_polls : kWaitPolls;
   ModParams mp = b->mp;
   int layout = b->layout;
   void* args[] = {&ba, &mp, &layout};
@@ -281,7 +237,8 @@ int bntt_batch_create(bntt_ctx* c, bntt_batch** out, bntt_plan* const* plans, si
   b->fast = arith_fast(c, plans[0]->fast);
   b->layout = plans[0]->layout;
   for (int m = 0; m <= 10; ++m) {
-    b->shapes.small[m] = batch_shape_for(m, MAP_CONTIG, 0);
+    const int tuned = tuned_batch_small_shape(m);
+    b->shapes.small[m] = tuned >= 0 ? tuned : batch_shape_for(m, MAP_CONTIG, 0);
     b->shapes.pass_il[m] = batch_shape_for(m, MAP_INTERLEAVED, 0);
     b->shapes.pass_contig[m] = batch_shape_for(m, MAP_CONTIG, 4);
     if (b->shapes.pass_contig[m] < 0) b->shapes.pass_contig[m] = batch_shape_for(m, MAP_CONTIG, 0);
@@ -308,14 +265,16 @@ int bntt_batch_run_dev(bntt_batch* b, const bntt_job* jobs, size_t count) {
   if (int rc = ctx_use_device(b->ctx)) return rc;
   b->last_launches = 0;
   if (count == 0) return BNTT_OK;
-  const bool same = b->last_jobs.size() == count && b->main.exec_stream == b->ctx->stream &&
+  const bool inject = b->inject_polls != 0;
+  const bool same = !inject && b->last_jobs.size() == count && b->main.exec_stream == b->ctx->stream &&
                     memcmp(b->last_jobs.data(), jobs, count * sizeof(bntt_job)) == 0;
   if (!same) {
     b->last_jobs.clear();
     if (int rc = build_schedule(b, b->main, jobs, count)) return rc;
     if (int rc = upload_and_capture(b, b->main, b->ctx->stream)) return rc;
-    b->last_jobs.assign(jobs, jobs + count);
+    if (!inject) b->last_jobs.assign(jobs, jobs + count);
   }
+  b->inject_polls = 0;  // an injected fault lasts one run
   return launch_schedule(b, b->main, b->ctx->stream);
 }
 
@@ -431,6 +390,62 @@ int bntt_batch_run_host(bntt_batch* b, const bntt_job* jobs, size_t count) {
 
 }  // extern "C"
 
+namespace bntt {
+
+int batch_shape_count() { return kNumShapes; }
+
+int batch_shape_info(int s, int* m, int* logr, int* tpc, int* map) {
+  *m = kShapes[s].m;
+  *logr = kShapes[s].logr;
+  *tpc = kShapes[s].tpc;
+  *map = kShapes[s].map;
+  return BNTT_OK;
+}
+
+// Median time of the persistent kernel over `count` contiguous transforms of
+// one plan with small-tile shape `shape` (autotuner measurement).
+int batch_time_uniform(bntt_ctx* c, bntt_plan* plan, int shape, size_t count, void* x, void* y,
+                       float* ms) {
+  bntt_batch* b = nullptr;
+  if (int rc = bntt_batch_create(c, &b, &plan, 1)) return rc;
+  b->shapes.small[plan->log2n] = shape;
+  count = std::min<size_t>(count, 65536);
+  const size_t bytes = (size_t)16 << plan->log2n;
+  std::vector<bntt_job> jobs(count);
+  for (size_t i = 0; i < count; ++i) {
+    jobs[i].x = static_cast<char*>(x) + i * bytes;
+    jobs[i].y = static_cast<char*>(y) + i * bytes;
+    jobs[i].plan = 0;
+    jobs[i].reserved = 0;
+  }
+  int rc = bntt_batch_run_dev(b, jobs.data(), count);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  std::vector<float> t;
+  if (!rc) {
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int r = 0; r < 5 && !rc; ++r) {
+      cudaEventRecord(e0, c->stream);
+      rc = bntt_batch_run_dev(b, jobs.data(), count);
+      cudaEventRecord(e1, c->stream);
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (!rc && e != cudaSuccess) rc = cuda_error(e, "autotune batch timing");
+      float v = 0;
+      cudaEventElapsedTime(&v, e0, e1);
+      t.push_back(v);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  bntt_batch_destroy(b);
+  if (rc) return rc;
+  std::sort(t.begin(), t.end());
+  *ms = t[t.size() / 2];
+  return BNTT_OK;
+}
+
+}  // namespace bntt
+
 // The plain per-call path over the same job list: every job is its own
 // forward transform, launched separately (one launch per transform of at most
 // 1024 points, one per HBM pass above).  This is the comparison point of the
@@ -531,11 +546,23 @@ extern "C" int bntt_batch_run_dev_noalloc(bntt_batch* b, const bntt_job* jobs, s
   ba.order = reinterpret_cast<const uint32_t*>(s + o_or);
   ba.ctl = reinterpret_cast<uint32_t*>(s + o_ctl);
   ba.pass_tiles = reinterpret_cast<const uint32_t*>(s + o_pt);
+  ba.wait_polls = kWaitPolls;
   ModParams mp = b->mp;
   int layout = b->layout;
   void* args[] = {&ba, &mp, &layout};
   BNTT_CK(cudaLaunchKernel(fn, dim3(grid), dim3(kBatchThreads), args, smem, st));
   c->launches++;
   b->last_launches = 1;
+  return BNTT_OK;
+}
+
+// Fault injection for tests of the failure path: the next bntt_batch_run_dev
+// makes every wait of a later HBM pass require one tile more than the earlier
+// pass has, and gives up after `poll_limit` polls (about 100 ns each).  The
+// kernel ends normally, the affected transforms are left incomplete, and
+// bntt_batch_status() reports BNTT_ETIMEOUT.  No GPU fault is involved.
+extern "C" int bntt_batch_inject_wait_timeout(bntt_batch* b, uint32_t poll_limit) {
+  BNTT_REQUIRE(b && poll_limit > 0, "NULL batch or zero poll limit");
+  b->inject_polls = poll_limit;
   return BNTT_OK;
 }

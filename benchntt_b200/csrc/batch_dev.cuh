@@ -84,7 +84,7 @@ constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 // control words: [0] queue head, [1] error word, [2 + 4*slot + p] pass counters
 constexpr int kCtlHeader = 2;
 constexpr int kMaxPasses = 4;
-// bounded wait: polls x ~100 ns sleeps, several seconds in all
+// bounded wait: default poll limit (polls x ~100 ns sleeps, a few seconds)
 constexpr uint32_t kWaitPolls = 1u << 25;
 
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
@@ -100,6 +100,7 @@ struct BatchArgs {
   const uint32_t* order;   // job indices sorted by size (SMALL tiles)
   uint32_t* ctl;
   const uint32_t* pass_tiles;  // [slot * kMaxPasses + p] tile count of pass p
+  uint32_t wait_polls;         // give up a dependency wait after this many polls
 };
 
 // One device function per shape (not inlined into the kernel's switch): keeps
@@ -145,7 +146,7 @@ __device__ __noinline__ void run_item(const WorkItem& it, const BatchArgs& ba, u
       uint32_t polls = 0;
       int ok = 1;
       while (ld_acquire(&counters[it.pass - 1]) < want) {
-        if (++polls > kWaitPolls) {
+        if (++polls > ba.wait_polls) {
           atomicOr(&ba.ctl[1], 1u);
           ok = 0;
           break;

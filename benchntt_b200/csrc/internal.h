@@ -61,6 +61,7 @@ struct SubKernel {
   size_t smem;  // dynamic shared memory bytes
   const void* fn;
   int max_blocks_per_sm;  // filled lazily
+  int minb;               // __launch_bounds__ minimum resident CTAs
 };
 
 const std::vector<SubKernel>& sub_kernels();
@@ -70,6 +71,10 @@ const SubKernel* pick_sub_kernel(int m, int map, int fast, int logr_pref = 0, in
 int launch_sub(bntt_ctx* ctx, const SubKernel* k, const void* geom, const ModParams& mp,
                int layout, cudaStream_t stream, int grid_cap = 0);
 int blocks_per_sm(const SubKernel* k);
+
+// Autotuner choices (nullptr / -1 when not tuned).
+const SubKernel* tuned_sub_kernel(int m, int map, int fast, int l);
+int tuned_batch_small_shape(int m);
 
 // Pass decomposition of a 2^n transform: sizes of HBM passes (each <= 10).
 std::vector<int> split_passes(int n);

@@ -36,7 +36,7 @@ enum : int { MAP_CONTIG = 0, MAP_INTERLEAVED = 1 };
 struct SubRef {
   const uint4* x;    // element j at x[j << L]
   uint4* y;          // element j at y[j << L]
-  const uint4* tw;   // table of the whole transform
+  const uint4* tw;   // table of the whole transform, limb order (LAYOUT_U128)
   uint32_t trow;     // 2^S0 + H
   uint32_t lshift;   // L
   bool valid;
@@ -144,7 +144,9 @@ struct NttTile {
         const int half = 1 << (r - 1 - t);
 #pragma unroll
         for (int u = 0; u < (1 << t); ++u) {
-          const U128 w = from_mem(__ldg(sr.tw + ((gt << t) + (uint32_t)u)), layout);
+          // tables are stored in limb order (LAYOUT_U128) by the plan
+          const uint4 tv = __ldg(sr.tw + ((gt << t) + (uint32_t)u));
+          const U128 w = U128{{tv.x, tv.y, tv.z, tv.w}};
 #pragma unroll
           for (int k = 0; k < half; ++k) {
             const int j = (u << (r - t)) | k;

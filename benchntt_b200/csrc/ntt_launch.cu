@@ -12,6 +12,7 @@ void append_fast_contig(std::vector<SubKernel>& v);
 void append_fast_contig_r4(std::vector<SubKernel>& v);
 void append_fast_il(std::vector<SubKernel>& v);
 void append_ref(std::vector<SubKernel>& v);
+void append_fast_occ(std::vector<SubKernel>& v);
 
 const std::vector<SubKernel>& sub_kernels() {
   static std::vector<SubKernel> v = [] {
@@ -20,6 +21,7 @@ const std::vector<SubKernel>& sub_kernels() {
     append_fast_contig_r4(r);
     append_fast_il(r);
     append_ref(r);
+    append_fast_occ(r);
     return r;
   }();
   return v;
@@ -92,14 +94,14 @@ int plan_choose_kernels(bntt_plan* p) {
     const int m = p->passes[i];
     const int l = n - s0 - m;
     const int map = l > 0 ? MAP_INTERLEAVED : MAP_CONTIG;
-    // the first registered shape that fits (interleaved tiles need TPC
-    // adjacent columns, so TPC <= 2^l)
-    const SubKernel* k = nullptr;
+    // the tuned shape if the autotuner ran, else the first registered shape
+    // that fits (interleaved tiles need TPC adjacent columns, so TPC <= 2^l)
+    const SubKernel* k = tuned_sub_kernel(m, map, fast ? 1 : 0, l);
     for (const SubKernel& c : sub_kernels()) {
+      if (k) break;
       if (c.m != m || c.map != map || c.fast != (fast ? 1 : 0)) continue;
       if (map == MAP_INTERLEAVED && (1 << l) < c.tpc) continue;
       k = &c;
-      break;
     }
     if (!k) return set_error(BNTT_EINVAL, "no kernel compiled for pass m=%d map=%d", m, map);
     p->kernels.push_back(k);

@@ -368,20 +368,33 @@ static int plan_create_common(bntt_ctx* c, bntt_plan** out, unsigned log2n, cons
   return BNTT_OK;
 }
 
+// Plans keep their table in limb order (LAYOUT_U128: the kernels' register
+// order), whatever the caller's layout, so no kernel reorders twiddle words.
 int bntt_plan_create(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bntt_modulus* m,
                      const void* twiddles, int layout) {
   BNTT_REQUIRE(twiddles, "twiddles is NULL");
   int rc = plan_create_common(c, out, log2n, m, layout);
   if (rc) return rc;
   bntt_plan* p = *out;
-  const size_t bytes = (size_t)16 << log2n;
+  const size_t n = (size_t)1 << log2n, bytes = n * 16;
   if ((rc = ctx_alloc(c, &p->tw, bytes)) != 0) {
     delete p;
     *out = nullptr;
     return rc;
   }
   p->own_tw = true;
-  cudaError_t e = cudaMemcpy(p->tw, twiddles, bytes, cudaMemcpyHostToDevice);
+  cudaError_t e;
+  if (layout == BNTT_LAYOUT_HILO) {
+    std::vector<uint64_t> t(2 * n);
+    const uint64_t* src = static_cast<const uint64_t*>(twiddles);
+    for (size_t i = 0; i < n; ++i) {
+      t[2 * i] = src[2 * i + 1];
+      t[2 * i + 1] = src[2 * i];
+    }
+    e = cudaMemcpy(p->tw, t.data(), bytes, cudaMemcpyHostToDevice);
+  } else {
+    e = cudaMemcpy(p->tw, twiddles, bytes, cudaMemcpyHostToDevice);
+  }
   if (e == cudaSuccess) rc = plan_choose_kernels(p);
   else rc = cuda_error(e, "cudaMemcpy(twiddles)");
   if (rc) {
@@ -392,15 +405,40 @@ int bntt_plan_create(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bntt_mo
   return rc;
 }
 
+// With a device table in U128 layout the plan uses it in place; a HILO table
+// is copied once into a plan-owned buffer with its two words swapped.
 int bntt_plan_create_dev(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bntt_modulus* m,
                          const void* twiddles_dev, int layout) {
   BNTT_REQUIRE(twiddles_dev && ((uintptr_t)twiddles_dev & 15) == 0,
                "twiddles_dev must be a 16-byte aligned device pointer");
   int rc = plan_create_common(c, out, log2n, m, layout);
   if (rc) return rc;
-  (*out)->tw = const_cast<void*>(twiddles_dev);
-  if ((rc = plan_choose_kernels(*out)) != 0) {
-    delete *out;
+  bntt_plan* p = *out;
+  if (layout == BNTT_LAYOUT_U128) {
+    p->tw = const_cast<void*>(twiddles_dev);
+  } else {
+    const size_t n = (size_t)1 << log2n;
+    if ((rc = ctx_alloc(c, &p->tw, n * 16)) != 0) {
+      delete p;
+      *out = nullptr;
+      return rc;
+    }
+    p->own_tw = true;
+    char* d = static_cast<char*>(p->tw);
+    const char* s = static_cast<const char*>(twiddles_dev);
+    cudaError_t e = cudaMemcpy2D(d, 16, s + 8, 16, 8, n, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy2D(d + 8, 16, s, 16, 8, n, cudaMemcpyDeviceToDevice);
+    if (e != cudaSuccess) {
+      rc = cuda_error(e, "cudaMemcpy2D(twiddles)");
+      ctx_free(c, p->tw);
+      delete p;
+      *out = nullptr;
+      return rc;
+    }
+  }
+  if ((rc = plan_choose_kernels(p)) != 0) {
+    if (p->own_tw) ctx_free(c, p->tw);
+    delete p;
     *out = nullptr;
   }
   return rc;

@@ -167,8 +167,8 @@ __device__ __forceinline__ void mul_128x128(const U128& a, const U128& b, uint32
 
 // r = P mod q for q = 2^124 - k, P < 2^248, k < 2^14.
 //   P = H*2^124 + L      ->  t = L + H*k            (< 2^139)
-//   t = H2*2^124 + L2    ->  u = L2 + H2*k          (< 2^124 + 2^29 < 2q)
-//   r = u >= q ? u - q : u, tested as bit 124 of u + k.
+//   t = H2*2^124 + L2    ->  r = L2 + H2*k          (< 2^124 + 2^29 < 2q)
+//   r >= q ? r - q : r, tested as bit 124 of r + k.
 __device__ __forceinline__ U128 reduce_pm124(const uint32_t p[8], uint32_t k) {
   const uint32_t h0 = __funnelshift_r(p[3], p[4], 28);
   const uint32_t h1 = __funnelshift_r(p[4], p[5], 28);
@@ -188,23 +188,28 @@ __device__ __forceinline__ U128 reduce_pm124(const uint32_t p[8], uint32_t k) {
       : "=&r"(t0), "=&r"(t1), "=&r"(t2), "=&r"(t3), "=&r"(t4)
       : "r"(h0), "r"(h1), "r"(h2), "r"(h3), "r"(k), "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(l3));
   const uint32_t u = __funnelshift_r(t3, t4, 28) * k;
-  uint32_t r0, r1, r2, r3, s0, s1, s2, s3;
-  asm("add.cc.u32  %0, %8, %12;\n\t"
-      "addc.cc.u32 %1, %9, 0;\n\t"
-      "addc.cc.u32 %2, %10, 0;\n\t"
-      "addc.u32    %3, %11, 0;\n\t"
-      "add.cc.u32  %4, %0, %13;\n\t"
-      "addc.cc.u32 %5, %1, 0;\n\t"
-      "addc.cc.u32 %6, %2, 0;\n\t"
-      "addc.u32    %7, %3, 0;\n\t"
-      : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3), "=&r"(s0), "=&r"(s1), "=&r"(s2), "=&r"(s3)
-      : "r"(t0), "r"(t1), "r"(t2), "r"(t3 & 0x0FFFFFFFu), "r"(u), "r"(k));
-  const bool ge = (s3 >> 28) != 0u;
   U128 r;
-  r.w[0] = ge ? s0 : r0;
-  r.w[1] = ge ? s1 : r1;
-  r.w[2] = ge ? s2 : r2;
-  r.w[3] = ge ? (s3 & 0x0FFFFFFFu) : r3;
+  asm("add.cc.u32  %0, %4, %8;\n\t"
+      "addc.cc.u32 %1, %5, 0;\n\t"
+      "addc.cc.u32 %2, %6, 0;\n\t"
+      "addc.u32    %3, %7, 0;\n\t"
+      : "=r"(r.w[0]), "=r"(r.w[1]), "=r"(r.w[2]), "=r"(r.w[3])
+      : "r"(t0), "r"(t1), "r"(t2), "r"(t3 & 0x0FFFFFFFu), "r"(u));
+  // r < 2^124 + 2^29 < 2q.  r >= q needs r's top limb >= q's (0x0FFFFFFF,
+  // since k < 2^14): for residues spread over [0, q) that is about one case
+  // in 2^28, so the exact test and subtraction sit behind a branch.
+  if (__builtin_expect(r.w[3] >= 0x0FFFFFFFu, 0)) {
+    uint32_t s0, s1, s2, s3;
+    asm("add.cc.u32  %0, %4, %8;\n\t"
+        "addc.cc.u32 %1, %5, 0;\n\t"
+        "addc.cc.u32 %2, %6, 0;\n\t"
+        "addc.u32    %3, %7, 0;\n\t"
+        : "=r"(s0), "=r"(s1), "=r"(s2), "=r"(s3)
+        : "r"(r.w[0]), "r"(r.w[1]), "r"(r.w[2]), "r"(r.w[3]), "r"(k));
+    if (s3 >> 28) {  // r + k >= 2^124, i.e. r >= q: r - q = r + k - 2^124
+      r.w[0] = s0; r.w[1] = s1; r.w[2] = s2; r.w[3] = s3 & 0x0FFFFFFFu;
+    }
+  }
   return r;
 }
 

@@ -126,8 +126,9 @@ int bntt_fill_uniform_dev(bntt_ctx *ctx, void *buf_dev, size_t count, uint64_t s
  * 1 <= log2n <= 24. */
 int bntt_plan_create(bntt_ctx *ctx, bntt_plan **plan, unsigned log2n, const bntt_modulus *m,
                      const void *twiddles, int layout);
-/* Same, with the table already in device memory (not copied; must outlive
- * the plan). */
+/* Same, with the table already in device memory.  A BNTT_LAYOUT_U128 table
+ * is used in place (not copied; it must outlive the plan); a HILO table is
+ * copied once into plan-owned memory in limb order. */
 int bntt_plan_create_dev(bntt_ctx *ctx, bntt_plan **plan, unsigned log2n,
                          const bntt_modulus *m, const void *twiddles_dev, int layout);
 int bntt_plan_destroy(bntt_plan *plan);
@@ -186,6 +187,11 @@ int bntt_batch_run_dev_noalloc(bntt_batch *batch, const bntt_job *jobs, size_t c
 /* Status of the last run: BNTT_OK, or BNTT_ETIMEOUT if a device-side wait
  * gave up (synchronises the stream). */
 int bntt_batch_status(bntt_batch *batch);
+/* Fault injection for tests of the failure path: the next
+ * bntt_batch_run_dev makes the waits of later HBM passes unreachable and gives
+ * up after `poll_limit` polls (about 100 ns each); the kernel still ends, and
+ * bntt_batch_status() then reports BNTT_ETIMEOUT.  One run only. */
+int bntt_batch_inject_wait_timeout(bntt_batch *batch, uint32_t poll_limit);
 /* Kernel launches the last run issued (graph replays count their kernels). */
 size_t bntt_batch_last_launches(bntt_batch *batch);
 
@@ -217,6 +223,96 @@ int bntt_axpy_host(bntt_ctx *ctx, void *c, const void *a, const void *b, bntt_u1
 
 /* Kernel launches issued by this context since creation (all entry points). */
 uint64_t bntt_ctx_launch_count(bntt_ctx *ctx);
+
+/* ---------------------------------------------------------------- serving */
+/* A request loop with continuous batching.  Requests (forward NTTs of any
+ * plan size, vvmul, axpy) name device-resident operands; the server admits
+ * them in arrival order while its output arena (the HBM budget) has room,
+ * packs the admitted NTTs of each launch into one persistent-kernel run and
+ * the BLAS ops next to it, and keeps up to `slots` launches in flight on
+ * separate streams, so requests that arrive while others run are admitted as
+ * slots and memory free up and their work overlaps on the device.  Each
+ * completion carries its output (in the arena, until released) and the
+ * arrival / admission / completion times.  The reference has no serving
+ * path (one call per process, src/ntt_scalar.c:630). */
+typedef struct bntt_server bntt_server;
+
+typedef struct bntt_server_config {
+    size_t hbm_budget;   /* bytes of the output arena; 0 = 32 GiB */
+    uint32_t slots;      /* launches in flight at once; 0 = 4 */
+    uint32_t max_batch;  /* most requests per launch; 0 = 4096 */
+} bntt_server_config;
+
+#define BNTT_REQ_NTT 0
+#define BNTT_REQ_VVMUL 1
+#define BNTT_REQ_AXPY 2
+
+typedef struct bntt_request {
+    uint32_t kind;      /* BNTT_REQ_* */
+    uint32_t plan;      /* NTT: index into the server's plans */
+    uint64_t len;       /* vvmul / axpy: number of elements */
+    const void *x;      /* NTT input, or BLAS operand a (device) */
+    const void *b;      /* BLAS operand b (device) */
+    bntt_u128 scalar;   /* axpy: c = a + scalar * b */
+    uint64_t tag;       /* returned in the completion */
+    double t_arrive;    /* server clock (s); <= 0 means "now" at submit */
+} bntt_request;
+
+typedef struct bntt_completion {
+    uint64_t tag;
+    void *y;            /* output in the arena (device); bntt_server_release it */
+    size_t bytes;
+    double t_arrive;    /* server clock, seconds */
+    double t_admit;
+    double t_done;
+    int status;
+} bntt_completion;
+
+typedef struct bntt_server_stats {
+    uint64_t submitted;
+    uint64_t completed;
+    uint64_t launches;        /* batch launches (each: one kernel + BLAS kernels) */
+    uint64_t admission_waits; /* times the head request waited for arena space */
+    size_t peak_bytes;        /* most arena bytes in use at once */
+} bntt_server_stats;
+
+/* `plans` (NTT sizes) share one modulus; BLAS requests use `blas_modulus`. */
+int bntt_server_create(bntt_ctx *ctx, bntt_server **srv, bntt_plan *const *plans, size_t nplans,
+                       const bntt_modulus *blas_modulus, const bntt_server_config *cfg);
+int bntt_server_destroy(bntt_server *srv);
+double bntt_server_clock(bntt_server *srv);
+/* Thread-safe.  A request larger than the whole arena is refused (EBUDGET). */
+int bntt_server_submit(bntt_server *srv, const bntt_request *req);
+/* Moves up to `cap` completions to `out`; *n gets the count. */
+int bntt_server_poll(bntt_server *srv, bntt_completion *out, size_t cap, size_t *n);
+int bntt_server_release(bntt_server *srv, void *y);
+/* Waits until every submitted request has completed. */
+int bntt_server_drain(bntt_server *srv);
+int bntt_server_get_stats(bntt_server *srv, bntt_server_stats *stats);
+/* Replays `n` requests at their t_arrive offsets (seconds from the start of
+ * the replay) and returns each one's latency (completion - arrival) and the
+ * wall time from the first arrival to the last completion.  serial = 0: the
+ * server's continuous batching; serial = 1: one call at a time in arrival
+ * order (each request alone, synchronised, the per-call path).  Outputs are
+ * released as they complete. */
+int bntt_server_replay(bntt_server *srv, const bntt_request *reqs, size_t n, int serial,
+                       double *latency_s, double *wall_s);
+
+/* ------------------------------------------------------------- autotuner */
+/* Times every compiled kernel shape for transform sizes 2^1..2^10 (register
+ * tile of 8 or 16 elements per thread = radix and number of shared-memory
+ * passes, transforms per CTA, two or three resident CTAs per SM), the strided
+ * first pass of large transforms, and the persistent kernel's tile shape per
+ * size, on this device; the fastest become the defaults of plans and batches
+ * created afterwards in this process.  Writes the choices to `path` if it is
+ * not NULL.  A few seconds; about 768 MiB of device memory while it runs.
+ * The reference fixes one scalar / SIMD code path per size at compile time
+ * (src/ntt_scalar.c:21, benchmark/run_ntt.sh); no counterpart there. */
+int bntt_autotune(bntt_ctx *ctx, const char *path);
+/* Installs choices saved by bntt_autotune (refused for another device). */
+int bntt_autotune_load(bntt_ctx *ctx, const char *path);
+/* Drops tuned choices; compiled defaults apply to new plans and batches. */
+int bntt_autotune_reset(void);
 
 /* ------------------------------------------------------------ diagnostics */
 /* Measured throughput of the 32-bit integer multiply-add pipe on this device

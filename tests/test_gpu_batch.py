@@ -200,3 +200,21 @@ def test_full_uneven_batch_matches_oracle(ctx):
     assert s.engine.status() == bn.OK
     assert np.array_equal(s.output(), s.expected(threads=16))
     s.close()
+
+
+def test_bounded_wait_reports_timeout_and_context_stays_usable(ctx):
+    """Failure path of the persistent kernel without any GPU fault: an injected
+    run whose later-pass waits can never be satisfied gives up after a short
+    poll limit, the kernel ends, status is BNTT_ETIMEOUT, and the next run on
+    the same context is correct."""
+    b = W.uneven_batch(seed=10, n_small=200, large=((12, 2),))
+    s = Setup(ctx, b)
+    jobs = s.jobs()
+    bn.check(bn.lib().bntt_batch_inject_wait_timeout(s.engine.handle, 2000))
+    s.engine.run_dev(jobs)
+    assert s.engine.status() == bn.ETIMEOUT
+    assert b"waited too long" in bn.lib().bntt_last_error()
+    s.engine.run_dev(jobs)             # next run: no injection, schedule rebuilt
+    assert s.engine.status() == bn.OK
+    assert np.array_equal(s.output(), s.expected())
+    s.close()
