@@ -66,40 +66,6 @@ def parse():
     return ap.parse_args()
 
 
-# --------------------------------------------------------------- distributed
-class Dist:
-    def __init__(self, want: int):
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.pg = None
-        if self.world > 1:
-            import datetime
-
-            import torch
-            import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                    device_id=torch.device("cuda", self.local))
-            self.pg = dist
-
-    def barrier(self):
-        if self.pg:
-            self.pg.barrier()
-
-    def max(self, v: float) -> float:
-        if not self.pg:
-            return v
-        import torch
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
-        return float(t.item())
-
-    def close(self):
-        if self.pg:
-            self.pg.destroy_process_group()
-
-
 # ------------------------------------------------------------------- clocks
 class ClockSampler:
     """SM clock, power and clock-event reasons polled through NVML (read only)
@@ -321,8 +287,9 @@ def run_ours(args, dist: Dist):
     pid = {n: i for i, n in enumerate(batch.sizes)}
     x = torch.empty((batch.total, 2), dtype=torch.int64, device=dev)
     y = torch.empty_like(x)
-    bn.check(L.bntt_fill_uniform_dev(ctx.handle, x.data_ptr(), batch.total, W.SEED_INPUT, 0,
-                                     ctypes.byref(mod), 0))
+    # each rank transforms its own inputs (weak scaling: same work per GPU)
+    bn.check(L.bntt_fill_uniform_dev(ctx.handle, x.data_ptr(), batch.total, W.SEED_INPUT + dist.rank,
+                                     0, ctypes.byref(mod), 0))
     engine = bn.Batch(ctx, [plans[n] for n in batch.sizes])
     offs = batch.offsets * 16
     jobs = bn.Batch.jobs([x.data_ptr() + int(o) for o in offs], [y.data_ptr() + int(o) for o in offs],
@@ -639,8 +606,9 @@ def run_reference(args, dist: Dist):
 
 
 def main():
+    from benchntt_b200.dist import Dist
     args = parse()
-    dist = Dist(args.gpus)
+    dist = Dist()
     try:
         if args.impl == "reference":
             res = run_reference(args, dist)
