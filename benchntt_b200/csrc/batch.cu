@@ -2,14 +2,24 @@
 // and the bntt_batch_* entry points.  Device code: batch_dev.cuh,
 // instantiated in batch_kfast.cu / batch_kref.cu.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "batch_host.h"
 
 namespace bntt {
 
-const void* batch_kernel_fast();
+const void* batch_kernel_fast_minb(int minb);
 const void* batch_kernel_ref();
+
+// Resident CTAs per SM the fast batch kernel is compiled for (2 or 3); the
+// autotuner may change it.  BNTT_BATCH_MINB overrides it at start-up.
+static int g_batch_minb = [] {
+  const char* e = getenv("BNTT_BATCH_MINB");
+  return (e && atoi(e) == 2) ? 2 : 3;
+}();
+int batch_minb() { return g_batch_minb; }
+void set_batch_minb(int m) { g_batch_minb = m == 2 ? 2 : 3; }
 
 size_t shape_smem(int s) {
   const BatchShape& b = kShapes[s];
@@ -52,7 +62,7 @@ void free_schedule(bntt_ctx* c, Schedule& s) {
   s.d_jobs_cap = s.d_order_cap = s.d_items_cap = s.d_ctl_cap = s.d_pass_tiles_cap = 0;
 }
 
-const void* batch_kernel(bool fast) { return fast ? batch_kernel_fast() : batch_kernel_ref(); }
+const void* batch_kernel(bool fast) { return fast ? batch_kernel_fast_minb(g_batch_minb) : batch_kernel_ref(); }
 
 int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count) {
   sc.djobs.resize(count);

@@ -21,6 +21,7 @@
 #pragma once
 #include "internal.h"
 #include "ntt_core.cuh"
+#include "ntt_engine.cuh"
 
 namespace bntt {
 
@@ -46,30 +47,27 @@ struct WorkItem {
 };
 static_assert(sizeof(WorkItem) == 16, "work item layout");
 
-// Shapes available to the persistent kernel: all have 256 threads.
+// Tile shapes of the persistent kernel (all 256 threads).  Sizes 2^1 and
+// 2^2 use unrolled one-thread tiles; every other size and both mappings run
+// on NttEngine<3> (8 elements per thread), whose code is shared by all of
+// them.  TPC = 256 / (threads per sub-transform).
 #define BNTT_BATCH_SHAPES(X)               \
   X(0, 1, 1, 256, MAP_CONTIG)              \
   X(1, 2, 2, 256, MAP_CONTIG)              \
   X(2, 3, 3, 256, MAP_CONTIG)              \
-  X(3, 4, 4, 256, MAP_CONTIG)              \
+  X(3, 4, 3, 128, MAP_CONTIG)              \
   X(4, 5, 3, 64, MAP_CONTIG)               \
   X(5, 6, 3, 32, MAP_CONTIG)               \
   X(6, 7, 3, 16, MAP_CONTIG)               \
   X(7, 8, 3, 8, MAP_CONTIG)                \
   X(8, 9, 3, 4, MAP_CONTIG)                \
   X(9, 10, 3, 2, MAP_CONTIG)               \
-  X(10, 5, 4, 128, MAP_CONTIG)             \
-  X(11, 6, 4, 64, MAP_CONTIG)              \
-  X(12, 7, 4, 32, MAP_CONTIG)              \
-  X(13, 8, 4, 16, MAP_CONTIG)              \
-  X(14, 9, 4, 8, MAP_CONTIG)               \
-  X(15, 10, 4, 4, MAP_CONTIG)              \
-  X(16, 5, 4, 128, MAP_INTERLEAVED)        \
-  X(17, 6, 4, 64, MAP_INTERLEAVED)         \
-  X(18, 7, 4, 32, MAP_INTERLEAVED)         \
-  X(19, 8, 4, 16, MAP_INTERLEAVED)         \
-  X(20, 9, 4, 8, MAP_INTERLEAVED)          \
-  X(21, 10, 4, 4, MAP_INTERLEAVED)
+  X(10, 5, 3, 64, MAP_INTERLEAVED)         \
+  X(11, 6, 3, 32, MAP_INTERLEAVED)         \
+  X(12, 7, 3, 16, MAP_INTERLEAVED)         \
+  X(13, 8, 3, 8, MAP_INTERLEAVED)          \
+  X(14, 9, 3, 4, MAP_INTERLEAVED)          \
+  X(15, 10, 3, 2, MAP_INTERLEAVED)
 
 struct BatchShape {
   int m, logr, tpc, map;
@@ -80,6 +78,22 @@ inline constexpr BatchShape kShapes[] = {
 #undef BNTT_SHAPE_ROW
 };
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+
+// the same table for device code: size and mapping of a shape id
+__device__ __forceinline__ void shape_of(int id, int* m, int* map) {
+  switch (id) {
+#define BNTT_SHAPE_DEV(sid, M, LOGR, TPC, MAP) \
+  case sid:                                    \
+    *m = M;                                    \
+    *map = MAP;                                \
+    break;
+    BNTT_BATCH_SHAPES(BNTT_SHAPE_DEV)
+#undef BNTT_SHAPE_DEV
+    default:
+      *m = 3;
+      *map = MAP_CONTIG;
+  }
+}
 
 // control words: [0] queue head, [1] error word, [2 + 4*slot + p] pass counters
 constexpr int kCtlHeader = 2;
@@ -103,15 +117,12 @@ struct BatchArgs {
   uint32_t wait_polls;         // give up a dependency wait after this many polls
 };
 
-// One device function per shape (not inlined into the kernel's switch): keeps
-// ptxas compile time linear in the number of shapes.
-template <int M, int LOGR, int TPC, int MAP, class Arith>
-__device__ __noinline__ void run_item(const WorkItem& it, const BatchArgs& ba, uint4* smem,
-                                         const ModParams& mp, int layout, int* s_flag) {
-  using T = NttTile<M, LOGR, TPC, MAP, Arith>;
-  static_assert(T::THREADS == kBatchThreads, "batch shapes use 256 threads");
-  const int tid = threadIdx.x;
-  const int sub = T::sub_of(tid), lane = T::lane_of(tid);
+// The sub-transform a work item hands to thread `sub` of the tile: a whole
+// small job, or one sub-transform of an HBM pass of a large job.  Returns
+// false when the item is a later pass whose wait for its predecessor gave up
+// (the error word is set; the tile is skipped).
+__device__ __forceinline__ bool item_subref(const WorkItem& it, const BatchArgs& ba, int m, int sub,
+                                            int* s_flag, SubRef* out) {
   if (it.kind == ITEM_SMALL) {
     SubRef sr;
     sr.valid = (uint32_t)sub < it.b;
@@ -121,27 +132,17 @@ __device__ __noinline__ void run_item(const WorkItem& it, const BatchArgs& ba, u
     sr.tw = j.tw;
     sr.trow = 1;
     sr.lshift = 0;
-    T::template run<LD_NC>(sr, sub, lane, smem, mp, layout);
-    return;
+    *out = sr;
+    return true;
   }
   const DevJob& j = ba.jobs[it.a];
-  // pass geometry of this job (same split as split_passes on the host)
   const int n = (int)j.log2n;
-  const int k = (n + 9) / 10;
+  const int k = (n + 9) / 10;  // the same split as split_passes on the host
   int s0 = 0;
   for (int p = 0; p < (int)it.pass; ++p) s0 += n / k + (p < n % k ? 1 : 0);
-  SubGeom g;
-  g.x = it.pass == 0 ? j.x : j.y;
-  g.y = j.y;
-  g.tw = j.tw;
-  g.n = (uint32_t)n;
-  g.s0 = (uint32_t)s0;
-  g.m = (uint32_t)M;
-  g.l = (uint32_t)(n - s0 - M);
-  g.nsub = 1ull << (n - M);
-  uint32_t* counters = ba.ctl + kCtlHeader + j.slot * kMaxPasses;
   if (it.wait) {
-    if (tid == 0) {
+    uint32_t* counters = ba.ctl + kCtlHeader + j.slot * kMaxPasses;
+    if (threadIdx.x == 0) {
       const uint32_t want = ba.pass_tiles[j.slot * kMaxPasses + it.pass - 1];
       uint32_t polls = 0;
       int ok = 1;
@@ -156,24 +157,66 @@ __device__ __noinline__ void run_item(const WorkItem& it, const BatchArgs& ba, u
       *s_flag = ok;
     }
     __syncthreads();
-    if (!*s_flag) {
-      __syncthreads();
-      return;
-    }
+    if (!*s_flag) return false;
   }
-  const SubRef sr = make_subref(g, (uint64_t)it.b + (uint64_t)sub);
-  if (it.pass == 0) T::template run<LD_NC>(sr, sub, lane, smem, mp, layout);
-  else T::template run<LD_CG>(sr, sub, lane, smem, mp, layout);
-  // publish this tile: every thread's stores, then one release increment
+  SubGeom g;
+  g.x = it.pass == 0 ? j.x : j.y;
+  g.y = j.y;
+  g.tw = j.tw;
+  g.n = (uint32_t)n;
+  g.s0 = (uint32_t)s0;
+  g.m = (uint32_t)m;
+  g.l = (uint32_t)(n - s0 - m);
+  g.nsub = 1ull << (n - m);
+  *out = make_subref(g, (uint64_t)it.b + (uint64_t)sub);
+  return true;
+}
+
+// A pass tile publishes its completion: every thread's stores, then one
+// release increment of the job's pass counter.
+__device__ __forceinline__ void item_publish(const WorkItem& it, const BatchArgs& ba) {
+  if (it.kind != ITEM_PASS) return;
   __syncthreads();
-  if (tid == 0) {
+  if (threadIdx.x == 0) {
+    const DevJob& j = ba.jobs[it.a];
     __threadfence();
-    atomicAdd(&counters[it.pass], 1u);
+    atomicAdd(&ba.ctl[kCtlHeader + j.slot * kMaxPasses + it.pass], 1u);
   }
 }
 
+// Sizes 2^1, 2^2: one thread per transform, fully unrolled.
+template <int M, class Arith>
+__device__ __noinline__ void run_item_tiny(const WorkItem& it, const BatchArgs& ba, uint4* smem,
+                                           const ModParams& mp, int layout, int* s_flag) {
+  using T = NttTile<M, M, kBatchThreads, MAP_CONTIG, Arith>;
+  const int sub = threadIdx.x;
+  SubRef sr;
+  if (!item_subref(it, ba, M, sub, s_flag, &sr)) return;
+  T::template run<LD_NC>(sr, sub, 0, smem, mp, layout);
+  item_publish(it, ba);
+}
+
+// Every other shape: the runtime-size engine.
 template <class Arith>
-__global__ void __launch_bounds__(kBatchThreads) k_batch(BatchArgs ba, ModParams mp, int layout) {
+__device__ __noinline__ void run_item_engine(const WorkItem& it, const BatchArgs& ba, uint4* smem,
+                                             const ModParams& mp, int layout, int* s_flag) {
+  using E = NttEngine<3, Arith>;
+  int m, map;
+  shape_of(it.shape, &m, &map);
+  int sub, lane;
+  E::place(threadIdx.x, m, map, kBatchThreads, &sub, &lane);
+  SubRef sr;
+  if (!item_subref(it, ba, m, sub, s_flag, &sr)) return;
+  if (it.kind == ITEM_PASS && it.pass > 0)
+    E::template run<LD_CG>(m, map, kBatchThreads, sr, sub, lane, smem, mp, layout);
+  else
+    E::template run<LD_NC>(m, map, kBatchThreads, sr, sub, lane, smem, mp, layout);
+  item_publish(it, ba);
+}
+
+// MINB: resident CTAs per SM requested from the compiler (register budget).
+template <class Arith, int MINB>
+__global__ void __launch_bounds__(kBatchThreads, MINB) k_batch(BatchArgs ba, ModParams mp, int layout) {
   extern __shared__ uint4 smem[];
   __shared__ uint32_t s_item;
   __shared__ int s_flag;
@@ -183,16 +226,9 @@ __global__ void __launch_bounds__(kBatchThreads) k_batch(BatchArgs ba, ModParams
     const uint32_t i = s_item;
     if (i >= ba.nitems) break;
     const WorkItem it = ba.items[i];
-    switch (it.shape) {
-#define BNTT_SHAPE_CASE(id, M, LOGR, TPC, MAP)                                  \
-  case id:                                                                      \
-    run_item<M, LOGR, TPC, MAP, Arith>(it, ba, smem, mp, layout, &s_flag);      \
-    break;
-      BNTT_BATCH_SHAPES(BNTT_SHAPE_CASE)
-#undef BNTT_SHAPE_CASE
-      default:
-        break;
-    }
+    if (it.shape == 0) run_item_tiny<1, Arith>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 1) run_item_tiny<2, Arith>(it, ba, smem, mp, layout, &s_flag);
+    else run_item_engine<Arith>(it, ba, smem, mp, layout, &s_flag);
     __syncthreads();  // smem and s_item are reused by the next item
   }
 }

@@ -1,6 +1,9 @@
-// batch_kfast.cu -- the persistent batch kernel with ArithFast.
+// batch_kfast.cu -- the persistent batch kernel with ArithFast, compiled for
+// two or three resident CTAs per SM (register budget 128 or 85 per thread).
 #include "batch_dev.cuh"
 
 namespace bntt {
-const void* batch_kernel_fast() { return (const void*)&k_batch<ArithFast>; }
+const void* batch_kernel_fast_minb(int minb) {
+  return minb == 2 ? (const void*)&k_batch<ArithFast, 2> : (const void*)&k_batch<ArithFast, 3>;
+}
 }  // namespace bntt

@@ -2,5 +2,5 @@
 #include "batch_dev.cuh"
 
 namespace bntt {
-const void* batch_kernel_ref() { return (const void*)&k_batch<ArithRef>; }
+const void* batch_kernel_ref() { return (const void*)&k_batch<ArithRef, 2>; }
 }  // namespace bntt
