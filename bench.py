@@ -63,6 +63,8 @@ def parse():
                     help="run one secondary benchmark alone (profiling captures)")
     ap.add_argument("--logn", type=int, default=10, help="size for --only uniform")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the autotuner (profiling captures: no tuning launches first)")
     return ap.parse_args()
 
 
@@ -270,9 +272,11 @@ def run_ours(args, dist: Dist):
     import tempfile
     tune_path = os.path.join(tempfile.mkdtemp(), "bntt.tune")
     t_tune = time.perf_counter()
-    ctx.autotune(tune_path)
+    tuned = []
+    if not args.no_tune:
+        ctx.autotune(tune_path)
+        tuned = [l.strip() for l in open(tune_path) if l.startswith(("sub ", "batch "))]
     tune_s = time.perf_counter() - t_tune
-    tuned = [l.strip() for l in open(tune_path) if l.startswith(("sub ", "batch "))]
 
     # ---------------------------------------------------- headline workload
     batch = W.uneven_batch()

@@ -96,7 +96,7 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
   for (uint32_t ji : large) {
     const DevJob& d = sc.djobs[ji];
     const int n = (int)d.log2n;
-    const std::vector<int> passes = split_passes(n);
+    const std::vector<int> passes = split_passes(n, kBatchMaxPass);
     BNTT_REQUIRE(passes.size() <= (size_t)kMaxPasses, "log2n %d needs too many passes", n);
     int s0 = 0;
     for (size_t p = 0; p < passes.size(); ++p) {

@@ -5,7 +5,8 @@
 //   SMALL   TPC transforms of one size 2^n <= 1024, taken from a list of
 //           jobs sorted by size (one sub-transform per job)
 //   PASS p  TPC sub-transforms of HBM pass p of one large transform
-//           (n > 10, passes from split_passes: e.g. 2^20 = 10 + 10)
+//           (n > 10, passes of at most kBatchMaxPass stages: 2^16 = 8 + 8,
+//           2^20 = 7 + 7 + 6, so strided passes keep >= 8 adjacent columns)
 // A CTA takes the next item with an atomic counter.  Queue order is: all
 // first passes of large jobs, then small tiles from the largest size down,
 // then later passes.  Pass p > 0 of a job reads what pass p-1 wrote, so its
@@ -26,6 +27,10 @@
 namespace bntt {
 
 constexpr int kBatchThreads = 256;
+// Largest HBM pass of a large transform in the persistent kernel: a strided
+// pass of 2^m points has 256 >> (m - 3) adjacent columns per tile, and at
+// least 8 (128 contiguous bytes per row) keep its loads coalesced.
+constexpr int kBatchMaxPass = 8;
 
 struct DevJob {
   const uint4* x;
@@ -137,7 +142,7 @@ __device__ __forceinline__ bool item_subref(const WorkItem& it, const BatchArgs&
   }
   const DevJob& j = ba.jobs[it.a];
   const int n = (int)j.log2n;
-  const int k = (n + 9) / 10;  // the same split as split_passes on the host
+  const int k = (n + kBatchMaxPass - 1) / kBatchMaxPass;  // split_passes(n, kBatchMaxPass)
   int s0 = 0;
   for (int p = 0; p < (int)it.pass; ++p) s0 += n / k + (p < n % k ? 1 : 0);
   if (it.wait) {

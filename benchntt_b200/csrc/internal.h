@@ -76,8 +76,9 @@ int blocks_per_sm(const SubKernel* k);
 const SubKernel* tuned_sub_kernel(int m, int map, int fast, int l);
 int tuned_batch_small_shape(int m);
 
-// Pass decomposition of a 2^n transform: sizes of HBM passes (each <= 10).
-std::vector<int> split_passes(int n);
+// Pass decomposition of a 2^n transform: sizes of HBM passes (each <= max_m).
+// Plans use max_m = 10; the persistent kernel uses kBatchMaxPass.
+std::vector<int> split_passes(int n, int max_m = 10);
 
 int launch_blas(bntt_ctx* ctx, int op, void* c, const void* a, const void* b, U128 x, size_t len,
                 const ModParams& mp, bool fast, int layout, cudaStream_t stream);

@@ -75,11 +75,11 @@ int launch_sub(bntt_ctx* ctx, const SubKernel* k, const void* geom, const ModPar
   return BNTT_OK;
 }
 
-// Balanced split of n stages into HBM passes of at most 10 stages each
+// Balanced split of n stages into HBM passes of at most `max_m` stages each
 // (a 2^10-point sub-transform is the largest that lives in one CTA).
-std::vector<int> split_passes(int n) {
+std::vector<int> split_passes(int n, int max_m) {
   std::vector<int> p;
-  const int k = (n + 9) / 10;
+  const int k = (n + max_m - 1) / max_m;
   for (int i = 0; i < k; ++i) p.push_back(n / k + (i < n % k ? 1 : 0));
   return p;
 }
