@@ -374,6 +374,10 @@ def run_ours(args, dist: Dist):
     result["blas"] = blas_bench(args, ctx, stream, peaks)
     # --------------------------------------------------------- uniform sizes
     result["uniform"] = uniform_bench(args, ctx, stream, imad_peak)
+    # --------------------------------- fused transform + pointwise product
+    result["fused_mul"] = fused_bench(args, ctx, stream)
+    # ------------------------------------------- NTT-friendly prime (negacyclic)
+    result["negacyclic"] = negacyclic_bench(args, ctx, stream, batch, value)
     # --------------------------------------------------------------- serving
     engine.close()
     del x, y
@@ -518,6 +522,102 @@ def uniform_bench(args, ctx, stream, imad_peak, sizes=range(4, 11)) -> dict:
         plan.close()
         del x, y
     return res
+
+
+def fused_bench(args, ctx, stream, sizes=(4, 7, 10, 16)) -> dict:
+    """y = vector_mul(ntt(x), b) for 2^26 elements per size: the fused call
+    (bntt_ntt_forward_mul_dev) against the transform followed by vvmul."""
+    import torch
+
+    import benchntt_b200 as bn
+    L = bn.lib()
+    mod = bn.modulus(Q_NTT, MU_NTT)
+    res = {}
+    total = 1 << 26
+    for logn in sizes:
+        n = 1 << logn
+        count = total // n
+        x = torch.empty((total, 2), dtype=torch.int64, device=ctx.device)
+        b = torch.empty_like(x)
+        y = torch.empty_like(x)
+        bn.check(L.bntt_fill_uniform_dev(ctx.handle, x.data_ptr(), total, 7, 0, ctypes.byref(mod), 0))
+        bn.check(L.bntt_fill_uniform_dev(ctx.handle, b.data_ptr(), total, 8, 0, ctypes.byref(mod), 0))
+        plan = bn.Plan(ctx, logn, Q_NTT, MU_NTT, bn.fill_uniform(2000 + logn, n, Q_NTT))
+
+        def two_step():
+            plan.forward(y, x, count)
+            bn.check(L.bntt_vvmul_dev(ctx.handle, y.data_ptr(), y.data_ptr(), b.data_ptr(), total,
+                                      ctypes.byref(mod), 0))
+
+        def one_step():
+            plan.forward_mul(y, x, b, True, count)
+
+        row = {}
+        for name, fn in (("ntt_then_vvmul_ms", two_step), ("fused_ms", one_step)):
+            for _ in range(3):
+                fn()
+            e0, e1 = cuda_events()
+            reps = max(5, args.steps // 4)
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            row[name] = e0.elapsed_time(e1) / reps
+        row["speedup"] = row["ntt_then_vvmul_ms"] / row["fused_ms"]
+        row["transforms"] = count
+        res[str(n)] = row
+        plan.close()
+        del x, b, y
+    return res
+
+
+def negacyclic_bench(args, ctx, stream, batch, headline_value) -> dict:
+    """The headline uneven batch in the NTT-friendly prime mode: prime
+    2^124 - (62*2^21 - 1) from bntt_ntt_prime, root-power tables generated on
+    the device (bntt_plan_create_negacyclic), same persistent kernel."""
+    import torch
+
+    import benchntt_b200 as bn
+    from benchntt_b200 import workloads as W
+
+    q, mu = bn.ntt_prime(21)
+    w = bn.root_of_unity(q, mu, 21)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plans = {n: bn.Plan.negacyclic(ctx, n, q, mu, bn.powmod(q, mu, w, 1 << (21 - n - 1)))
+             for n in batch.sizes}
+    ctx.synchronize()
+    plan_s = time.perf_counter() - t0
+    pid = {n: i for i, n in enumerate(batch.sizes)}
+    dev = torch.cuda.current_device()
+    x = torch.empty((batch.total, 2), dtype=torch.int64, device=dev)
+    y = torch.empty_like(x)
+    bn.check(bn.lib().bntt_fill_uniform_dev(ctx.handle, x.data_ptr(), batch.total, W.SEED_INPUT, 0,
+                                            ctypes.byref(bn.modulus(q, mu)), 0))
+    engine = bn.Batch(ctx, [plans[n] for n in batch.sizes])
+    offs = batch.offsets * 16
+    jobs = bn.Batch.jobs([x.data_ptr() + int(o) for o in offs], [y.data_ptr() + int(o) for o in offs],
+                         [pid[int(n)] for n in batch.logns])
+    for _ in range(max(3, args.warmup)):
+        engine.run_dev(jobs)
+    e0, e1 = cuda_events()
+    reps = max(5, args.steps // 2)
+    e0.record(stream)
+    for _ in range(reps):
+        engine.run_dev(jobs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if engine.status() != bn.OK:
+        raise RuntimeError("batch kernel reported a timed-out wait")
+    ms = e0.elapsed_time(e1) / reps
+    engine.close()
+    for p in plans.values():
+        p.close()
+    return {"modulus": f"2^124 - {(1 << 124) - q:#x} (2^21 | q - 1)", "value": batch.count / (ms * 1e-3),
+            "unit": UNIT, "ms_per_step": ms, "vs_reference_modulus": batch.count / (ms * 1e-3) / headline_value,
+            "plan_create_s": plan_s, "tables": "T[k] = psi^brv(k), generated on the device",
+            "parity": "tests/test_gpu_negacyclic.py (reference ntt() fixtures, 2^2..2^20)"}
 
 
 def serving_bench(args, ctx) -> dict:

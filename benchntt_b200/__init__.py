@@ -120,9 +120,15 @@ _SIGS = [
     ("bntt_plan_create", _I, [_P, ctypes.POINTER(_P), _U, _PM, _P, _I]),
     ("bntt_plan_create_dev", _I, [_P, ctypes.POINTER(_P), _U, _PM, _P, _I]),
     ("bntt_plan_destroy", _I, [_P]),
+    ("bntt_ntt_prime", _I, [_U, _PM]),
+    ("bntt_root_of_unity", _I, [_PM, _U, ctypes.POINTER(U128)]),
+    ("bntt_powmod", _I, [_PM, U128, U128, ctypes.POINTER(U128)]),
+    ("bntt_twiddles_negacyclic", _I, [_PM, _U, U128, _P, _I]),
+    ("bntt_plan_create_negacyclic", _I, [_P, ctypes.POINTER(_P), _U, _PM, U128, _I]),
     ("bntt_plan_log2n", _U, [_P]),
     ("bntt_ntt_forward_dev", _I, [_P, _P, _P, _S]),
     ("bntt_ntt_forward_host", _I, [_P, _P, _P, _S]),
+    ("bntt_ntt_forward_mul_dev", _I, [_P, _P, _P, _P, _I, _S]),
     ("bntt_batch_create", _I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _S]),
     ("bntt_batch_destroy", _I, [_P]),
     ("bntt_batch_run_dev", _I, [_P, ctypes.POINTER(JobC), _S]),
@@ -184,6 +190,38 @@ def modulus(q: int, mu: int | None = None) -> ModulusC:
     if mu is None:
         mu = (1 << 251) // q
     return ModulusC(U128.of(q), U128.of(mu))
+
+
+# ------------------------------------------------- NTT-friendly prime mode
+def ntt_prime(log2_order: int) -> tuple[int, int]:
+    """(q, mu): q = 2^124 - (c*2^log2_order - 1), smallest c giving a prime
+    (Miller-Rabin, bntt_ntt_prime), mu = floor(2^251 / q)."""
+    m = ModulusC()
+    check(lib().bntt_ntt_prime(log2_order, ctypes.byref(m)))
+    return (m.q.hi << 64) | m.q.lo, (m.mu.hi << 64) | m.mu.lo
+
+
+def root_of_unity(q: int, mu: int, log2_order: int) -> int:
+    """A primitive 2^log2_order-th root of unity mod q."""
+    r = U128()
+    check(lib().bntt_root_of_unity(ctypes.byref(modulus(q, mu)), log2_order, ctypes.byref(r)))
+    return (r.hi << 64) | r.lo
+
+
+def powmod(q: int, mu: int, a: int, e: int) -> int:
+    r = U128()
+    check(lib().bntt_powmod(ctypes.byref(modulus(q, mu)), U128.of(a), U128.of(e),
+                            ctypes.byref(r)))
+    return (r.hi << 64) | r.lo
+
+
+def twiddles_negacyclic(q: int, mu: int, log2n: int, psi: int,
+                        layout: int = LAYOUT_HILO) -> np.ndarray:
+    """Host table T[k] = psi^brv(k) (T[0] = 1) as an (N, 2) uint64 array."""
+    t = np.empty((1 << log2n, 2), dtype=np.uint64)
+    check(lib().bntt_twiddles_negacyclic(ctypes.byref(modulus(q, mu)), log2n, U128.of(psi),
+                                         t.ctypes.data, layout))
+    return t
 
 
 # ------------------------------------------------------------------ helpers
@@ -293,6 +331,20 @@ class Plan:
             check(lib().bntt_plan_create(ctx.handle, ctypes.byref(self._h), log2n,
                                          ctypes.byref(self._m), _host_ptr(tw), layout))
 
+    @classmethod
+    def negacyclic(cls, ctx: Context, log2n: int, q: int, mu: int, psi: int,
+                   layout: int = LAYOUT_HILO) -> "Plan":
+        """Plan whose table T[k] = psi^brv(k) is generated on the device
+        (bntt_plan_create_negacyclic): the network then computes the
+        negacyclic NTT, outputs in bit-reversed order."""
+        self = cls.__new__(cls)
+        self.ctx, self.log2n, self.q, self.mu, self.layout = ctx, log2n, q, mu, layout
+        self._m = modulus(q, mu)
+        self._h = ctypes.c_void_p()
+        check(lib().bntt_plan_create_negacyclic(ctx.handle, ctypes.byref(self._h), log2n,
+                                                ctypes.byref(self._m), U128.of(psi), layout))
+        return self
+
     @property
     def handle(self):
         return self._h
@@ -305,6 +357,14 @@ class Plan:
         else:
             b = batch if batch is not None else x.size // (2 * n)
             check(lib().bntt_ntt_forward_host(self._h, _host_ptr(y), _host_ptr(x), b))
+
+    def forward_mul(self, y, x, b, per_transform: bool = True, batch: int | None = None) -> None:
+        """y = ntt(x) o b in one launch sequence (bntt_ntt_forward_mul_dev);
+        device tensors only."""
+        n = 1 << self.log2n
+        bt = batch if batch is not None else x.numel() // (2 * n)
+        check(lib().bntt_ntt_forward_mul_dev(self._h, _dev_ptr(y), _dev_ptr(x), _dev_ptr(b),
+                                             1 if per_transform else 0, bt))
 
     def close(self) -> None:
         if self._h:

@@ -128,5 +128,9 @@ int ctx_free(bntt_ctx* ctx, void* p);
 int ctx_use_device(bntt_ctx* ctx);
 bool arith_fast(bntt_ctx* ctx, bool modulus_fast);
 int plan_choose_kernels(bntt_plan* p);
-int ntt_forward_on(bntt_plan* plan, void* y, const void* x, size_t batch, cudaStream_t s);
+int plan_create_common(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bntt_modulus* m,
+                       int layout);
+// b != nullptr fuses y = y * b into the last pass (MulB in ntt_core.cuh).
+int ntt_forward_on(bntt_plan* plan, void* y, const void* x, size_t batch, cudaStream_t s,
+                   const void* b = nullptr, uint64_t bmask = 0);
 }  // namespace bntt

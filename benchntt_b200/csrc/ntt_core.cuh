@@ -52,6 +52,17 @@ __device__ __forceinline__ uint4 ld_data(const uint4* p) {
   else return __ldg(p);
 }
 
+// Optional pointwise product fused into the store of a transform's last
+// pass: element e of y becomes y[e] * b[e'] mod q (vector_mul,
+// src/blas_scalar.c:594), e' = (e's offset from ybase) & bmask.  bmask = N - 1
+// applies one vector to every transform of the batch; all ones pairs
+// transform t with b's t-th vector.  b == nullptr: plain store.
+struct MulB {
+  const uint4* b = nullptr;
+  const uint4* ybase = nullptr;
+  uint64_t bmask = 0;
+};
+
 template <int M, int LOGR, int TPC, int MAP, class Arith>
 struct NttTile {
   static constexpr int R = 1 << LOGR;
@@ -97,14 +108,16 @@ struct NttTile {
   // zeros and store nothing.
   template <int LDP>
   __device__ __forceinline__ static void run(const SubRef& sr, int sub, int lane, uint4* smem,
-                                             const ModParams& mp, int layout) {
+                                             const ModParams& mp, int layout,
+                                             const MulB& mb = MulB{}) {
     U128 v[R];
-    pass<0, LDP>(v, sr, sub, lane, smem, mp, layout);
+    pass<0, LDP>(v, sr, sub, lane, smem, mp, layout, mb);
   }
 
   template <int P, int LDP>
   __device__ __forceinline__ static void pass(U128 (&v)[R], const SubRef& sr, int sub, int lane,
-                                              uint4* smem, const ModParams& mp, int layout) {
+                                              uint4* smem, const ModParams& mp, int layout,
+                                              const MulB& mb) {
     constexpr int r = bits(P);
     constexpr int s0 = start(P);
     constexpr int lo = M - s0 - r;        // lowest local bit this pass touches
@@ -165,7 +178,15 @@ struct NttTile {
       for (int j = 0; j < G; ++j) {
         const int idx = base | (j << lo);
         if constexpr (P == NPASS - 1) {
-          if (sr.valid) sr.y[(size_t)idx << sr.lshift] = to_mem(v[i * G + j], layout);
+          if (sr.valid) {
+            uint4* yp = sr.y + ((size_t)idx << sr.lshift);
+            U128 o = v[i * G + j];
+            if (mb.b) {
+              const uint4 bv = __ldg(mb.b + ((uint64_t)(yp - mb.ybase) & mb.bmask));
+              o = Arith::mul(o, from_mem(bv, layout), mp);
+            }
+            *yp = to_mem(o, layout);
+          }
         } else {
           const U128& e = v[i * G + j];
           smem[slot(sub, idx)] = make_uint4(e.w[0], e.w[1], e.w[2], e.w[3]);
@@ -174,7 +195,7 @@ struct NttTile {
     }
     if constexpr (P + 1 < NPASS) {
       sync();
-      pass<P + 1, LDP>(v, sr, sub, lane, smem, mp, layout);
+      pass<P + 1, LDP>(v, sr, sub, lane, smem, mp, layout, mb);
     }
   }
 };
@@ -189,6 +210,8 @@ struct SubGeom {
   uint32_t m;       // stages in this pass
   uint32_t l;       // low bits below the pass bits
   uint64_t nsub;    // number of sub-transforms (all transforms of the batch)
+  const uint4* b = nullptr;  // last pass only: fused pointwise product (MulB)
+  uint64_t bmask = 0;
 };
 
 // Sub-transform `sid` of a geometry: sid = (transform << (S0 + L)) | (H << L) | c.

@@ -19,7 +19,7 @@ __global__ void __launch_bounds__(NttTile<M, LOGR, TPC, MAP, Arith>::THREADS, MI
   const uint64_t ntiles = (g.nsub + TPC - 1) / TPC;
   for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const SubRef sr = make_subref(g, tile * TPC + (uint64_t)sub);
-    T::template run<LD_NC>(sr, sub, lane, smem, mp, layout);
+    T::template run<LD_NC>(sr, sub, lane, smem, mp, layout, MulB{g.b, g.y, g.bmask});
     if constexpr (T::NPASS > 1) T::sync();  // smem is reused by the next tile
   }
 }

@@ -110,7 +110,8 @@ int plan_choose_kernels(bntt_plan* p) {
   return BNTT_OK;
 }
 
-int ntt_forward_on(bntt_plan* plan, void* y, const void* x, size_t batch, cudaStream_t s) {
+int ntt_forward_on(bntt_plan* plan, void* y, const void* x, size_t batch, cudaStream_t s,
+                   const void* b, uint64_t bmask) {
   if (batch == 0) return BNTT_OK;
   const int n = (int)plan->log2n;
   int s0 = 0;
@@ -125,6 +126,10 @@ int ntt_forward_on(bntt_plan* plan, void* y, const void* x, size_t batch, cudaSt
     g.m = (uint32_t)m;
     g.l = (uint32_t)(n - s0 - m);
     g.nsub = (uint64_t)batch << (n - m);
+    if (i + 1 == plan->passes.size()) {
+      g.b = static_cast<const uint4*>(b);
+      g.bmask = bmask;
+    }
     int rc = launch_sub(plan->ctx, plan->kernels[i], &g, plan->mp, plan->layout, s);
     if (rc) return rc;
     s0 += m;

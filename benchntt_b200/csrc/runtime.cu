@@ -47,15 +47,17 @@ u128 barrett_mu(u128 q) {
 }
 
 // The pseudo-Mersenne multiply equals the reference mulmod128 when
-//   2^123 < q = 2^124 - k,  1 <= k < 2^14,  mu = floor(2^251 / q):
-// for operands below 2^124 the reference's intermediate sums cannot wrap, its
-// quotient estimate is floor(P/q) or one less (the estimate loses less than
-// 2^122/q + 1/8 < 1), so one conditional subtraction returns P mod q.
+//   2^123 < q = 2^124 - k,  1 <= k < 2^31,  mu = floor(2^251 / q):
+// for operands below 2^124 the reference's intermediate sums cannot wrap
+// (mu = 2^127 + d with d < 2^35, so its mulhi128 cross terms stay below
+// 2^128), and its quotient estimate is floor(P/q) or one less (the two
+// truncations lose less than 2^122/q + P/2^251 < 1/2 + 1/8), so one
+// conditional subtraction returns P mod q.
 bool modulus_fast(u128 q, u128 mu, uint32_t* k_out) {
   const u128 top = (u128)1 << 124;
   if (q >= top || q <= ((u128)1 << 123)) return false;
   const u128 k = top - q;
-  if (k >= (1u << 14)) return false;
+  if (k >= ((u128)1 << 31)) return false;
   if (mu != barrett_mu(q)) return false;
   if (k_out) *k_out = (uint32_t)k;
   return true;
@@ -320,6 +322,24 @@ int launch_fill(bntt_ctx* ctx, void* buf, size_t count, uint64_t seed, uint64_t 
   return BNTT_OK;
 }
 
+// Fields shared by every plan constructor; the table is set by the caller.
+int plan_create_common(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bntt_modulus* m,
+                       int layout) {
+  BNTT_REQUIRE(c && out && m, "NULL argument");
+  *out = nullptr;
+  BNTT_REQUIRE(log2n >= 1 && log2n <= 24, "log2n %u outside [1, 24]", log2n);
+  BNTT_REQUIRE(layout == BNTT_LAYOUT_HILO || layout == BNTT_LAYOUT_U128, "bad layout %d", layout);
+  if (int rc = ctx_use_device(c)) return rc;
+  auto* p = new bntt_plan();
+  p->ctx = c;
+  p->log2n = log2n;
+  p->mod = *m;
+  p->layout = layout;
+  p->mp = make_params(*m, &p->fast);
+  *out = p;
+  return BNTT_OK;
+}
+
 }  // namespace bntt
 
 extern "C" {
@@ -351,29 +371,13 @@ int bntt_fill_uniform_dev(bntt_ctx* c, void* buf, size_t count, uint64_t seed, u
 }
 
 // -------------------------------------------------------------------- NTT
-static int plan_create_common(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bntt_modulus* m,
-                              int layout) {
-  BNTT_REQUIRE(c && out && m, "NULL argument");
-  *out = nullptr;
-  BNTT_REQUIRE(log2n >= 1 && log2n <= 24, "log2n %u outside [1, 24]", log2n);
-  BNTT_REQUIRE(layout == BNTT_LAYOUT_HILO || layout == BNTT_LAYOUT_U128, "bad layout %d", layout);
-  if (int rc = ctx_use_device(c)) return rc;
-  auto* p = new bntt_plan();
-  p->ctx = c;
-  p->log2n = log2n;
-  p->mod = *m;
-  p->layout = layout;
-  p->mp = make_params(*m, &p->fast);
-  *out = p;
-  return BNTT_OK;
-}
 
 // Plans keep their table in limb order (LAYOUT_U128: the kernels' register
 // order), whatever the caller's layout, so no kernel reorders twiddle words.
 int bntt_plan_create(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bntt_modulus* m,
                      const void* twiddles, int layout) {
   BNTT_REQUIRE(twiddles, "twiddles is NULL");
-  int rc = plan_create_common(c, out, log2n, m, layout);
+  int rc = bntt::plan_create_common(c, out, log2n, m, layout);
   if (rc) return rc;
   bntt_plan* p = *out;
   const size_t n = (size_t)1 << log2n, bytes = n * 16;
@@ -411,7 +415,7 @@ int bntt_plan_create_dev(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bnt
                          const void* twiddles_dev, int layout) {
   BNTT_REQUIRE(twiddles_dev && ((uintptr_t)twiddles_dev & 15) == 0,
                "twiddles_dev must be a 16-byte aligned device pointer");
-  int rc = plan_create_common(c, out, log2n, m, layout);
+  int rc = bntt::plan_create_common(c, out, log2n, m, layout);
   if (rc) return rc;
   bntt_plan* p = *out;
   if (layout == BNTT_LAYOUT_U128) {
@@ -465,6 +469,23 @@ int bntt_ntt_forward_dev(bntt_plan* p, void* y, const void* x, size_t batch) {
   BNTT_REQUIRE(aligned16(x) && aligned16(y), "device buffers must be 16-byte aligned");
   if (int rc = ctx_use_device(p->ctx)) return rc;
   return ntt_forward_on(p, y, x, batch, p->ctx->stream);
+}
+
+int bntt_ntt_forward_mul_dev(bntt_plan* p, void* y, const void* x, const void* b,
+                             int b_per_transform, size_t batch) {
+  BNTT_REQUIRE(p, "plan is NULL");
+  if (batch == 0) return BNTT_OK;
+  BNTT_REQUIRE(x && y && b, "NULL buffer");
+  BNTT_REQUIRE(aligned16(x) && aligned16(y) && aligned16(b),
+               "device buffers must be 16-byte aligned");
+  BNTT_REQUIRE(b_per_transform == 0 || b_per_transform == 1, "b_per_transform must be 0 or 1");
+  const size_t n = (size_t)1 << p->log2n;
+  const uintptr_t y0 = (uintptr_t)y, y1 = y0 + batch * n * 16;
+  const uintptr_t b0 = (uintptr_t)b, b1 = b0 + (b_per_transform ? batch : 1) * n * 16;
+  BNTT_REQUIRE(b1 <= y0 || b0 >= y1, "b must not overlap y");
+  if (int rc = ctx_use_device(p->ctx)) return rc;
+  return ntt_forward_on(p, y, x, batch, p->ctx->stream, b,
+                        b_per_transform ? ~0ull : (uint64_t)(n - 1));
 }
 
 }  // extern "C"

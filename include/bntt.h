@@ -66,8 +66,9 @@ typedef struct bntt_modulus {
 #define BNTT_LAYOUT_U128 1
 
 /* Arithmetic selection.
- * AUTO: a pseudo-Mersenne multiply when q = 2^124 - k (k < 2^14) and
- *       mu = floor(2^251/q) -- both reference moduli -- for which the
+ * AUTO: a pseudo-Mersenne multiply when q = 2^124 - k (k < 2^31) and
+ *       mu = floor(2^251/q) -- both reference moduli and the NTT-friendly
+ *       primes of bntt_ntt_prime -- for which the
  *       reference's Barrett reduction provably returns a*b mod q exactly;
  *       otherwise the replica below.
  * REFERENCE: a word-for-word replica of mulmod128 (src/ntt_scalar.c:173-199),
@@ -134,6 +135,33 @@ int bntt_plan_create_dev(bntt_ctx *ctx, bntt_plan **plan, unsigned log2n,
 int bntt_plan_destroy(bntt_plan *plan);
 unsigned bntt_plan_log2n(const bntt_plan *plan);
 
+/* NTT-friendly prime mode.  The reference's tables are arbitrary constants
+ * (data/twd_N.txt; 2^124 - 719 has no 2-power roots of unity), but ntt()
+ * takes modulus, mu and table at run time (src/ntt_scalar.c:582), so the same
+ * network computes the negacyclic transform
+ *     Y[i] = sum_j X[j] * psi^((2*brv(i) + 1) * j)  mod q
+ * (outputs in bit-reversed order; brv reverses log2 N bits) when q has
+ * 2N | q - 1, psi is a primitive 2N-th root of unity and
+ *     T[k] = psi^brv(k)  (k = 1..N-1;  T[0] = 1, never read).
+ *
+ * bntt_ntt_prime: q = 2^124 - (c*2^log2_order - 1) for the smallest c >= 1
+ *   that passes a Miller-Rabin test to the first 24 prime bases, with
+ *   mu = floor(2^251/q); k = 2^124 - q < 2^31, so the default fast multiply
+ *   applies.  EINVAL if no such prime exists.
+ * bntt_root_of_unity: a primitive 2^log2_order-th root of unity mod q
+ *   (g^((q-1)/2^log2_order) for the smallest g >= 2 of that exact order).
+ * bntt_powmod: a^e mod q (host, exact) for 2^123 < q < 2^124.
+ * bntt_twiddles_negacyclic: the table above on the host (2^log2n elements).
+ * bntt_plan_create_negacyclic: a plan whose table is generated on the device
+ *   from psi (no host table, no upload); q must take the fast multiply. */
+int bntt_ntt_prime(unsigned log2_order, bntt_modulus *m);
+int bntt_root_of_unity(const bntt_modulus *m, unsigned log2_order, bntt_u128 *root);
+int bntt_powmod(const bntt_modulus *m, bntt_u128 a, bntt_u128 e, bntt_u128 *out);
+int bntt_twiddles_negacyclic(const bntt_modulus *m, unsigned log2n, bntt_u128 psi, void *table,
+                             int layout);
+int bntt_plan_create_negacyclic(bntt_ctx *ctx, bntt_plan **plan, unsigned log2n,
+                                const bntt_modulus *m, bntt_u128 psi, int layout);
+
 /* Forward transform of `batch` contiguous inputs (replaces ntt(),
  * src/ntt_scalar.c:582).  y may equal x.  One launch for 2^log2n <= 1024,
  * one launch per HBM pass above. */
@@ -141,6 +169,16 @@ int bntt_ntt_forward_dev(bntt_plan *plan, void *y, const void *x, size_t batch);
 /* Host-pointer form: copies in, transforms, copies out (the reference's
  * call shape; pipelined over chunks of the batch). */
 int bntt_ntt_forward_host(bntt_plan *plan, void *y, const void *x, size_t batch);
+/* Transform fused with the pointwise product that follows it in a
+ * polynomial-multiply pipeline:  y_t = vector_mul(ntt(x_t), b_t)
+ * (src/ntt_scalar.c:582 then src/blas_scalar.c:594) under the plan's
+ * modulus, with the product applied as the last pass stores, so the
+ * transform's output never makes a second trip through HBM.
+ * b_per_transform = 1: b holds `batch` vectors of 2^log2n elements, one per
+ * transform; 0: one vector applied to every transform.  y may equal x; b may
+ * equal x but must not overlap y.  Same layout for x, y and b. */
+int bntt_ntt_forward_mul_dev(bntt_plan *plan, void *y, const void *x, const void *b,
+                             int b_per_transform, size_t batch);
 
 /* ------------------------------------------------------- mixed-size batch */
 /* One transform of a mixed batch: x and y are device pointers (or host

@@ -265,3 +265,102 @@ def edge_values(q: int) -> list[int]:
             q - (1 << 64), q - (1 << 64) + 1, lo(q), lo(q) + 1, hi(q) << 64,
             (hi(q) << 64) - 1, q >> 1, (q >> 1) + 1, (1 << 123), (1 << 123) - 1}
     return sorted(v for v in vals if 0 <= v <= q)
+
+
+# ------------------------------------------------- NTT-friendly prime mode
+# Pure-Python restatement (independent of libbntt) used to pin
+# bntt_ntt_prime / bntt_root_of_unity / bntt_twiddles_negacyclic and to
+# build the negacyclic fixtures from the compiled reference ntt().
+MR_BASES = (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61, 67, 71, 73,
+            79, 83, 89)
+NC_LOG2_ORDER = 21   # 2^21 | q - 1: negacyclic transforms up to N = 2^20
+
+
+def is_probable_prime(n: int) -> bool:
+    for p in MR_BASES:
+        if n % p == 0:
+            return n == p
+    d, s = n - 1, 0
+    while d % 2 == 0:
+        d //= 2
+        s += 1
+    for a in MR_BASES:
+        x = pow(a, d, n)
+        if x in (1, n - 1):
+            continue
+        for _ in range(s - 1):
+            x = x * x % n
+            if x == n - 1:
+                break
+        else:
+            return False
+    return True
+
+
+def ntt_prime_py(log2_order: int) -> int:
+    """Smallest-c prime 2^124 - (c*2^log2_order - 1) with k < 2^31."""
+    c = 1
+    while True:
+        k = (c << log2_order) - 1
+        assert k < 1 << 31, "no prime in range"
+        if is_probable_prime((1 << 124) - k):
+            return (1 << 124) - k
+        c += 1
+
+
+def root_of_unity_py(q: int, log2_order: int) -> int:
+    for g in range(2, 4096):
+        w = pow(g, (q - 1) >> log2_order, q)
+        if pow(w, 1 << (log2_order - 1), q) == q - 1:
+            return w
+    raise ValueError("no root found")
+
+
+def brv(k: int, n: int) -> int:
+    return int(format(k, f"0{n}b")[::-1], 2) if n else 0
+
+
+def negacyclic_table(q: int, logn: int, psi: int) -> np.ndarray:
+    """T[k] = psi^brv(k), T[0] = 1, as (N, 2) hi-first pairs."""
+    n = 1 << logn
+    pw = [1] * n
+    for j in range(1, n):
+        pw[j] = pw[j - 1] * psi % q
+    return to_pairs([pw[brv(k, logn)] for k in range(n)])
+
+
+def negacyclic_psi(q: int, logn: int, log2_order: int = NC_LOG2_ORDER) -> int:
+    """Primitive 2N-th root: the order-2^log2_order root to the 2^(order-n-1)."""
+    w = root_of_unity_py(q, log2_order)
+    return pow(w, 1 << (log2_order - logn - 1), q)
+
+
+def negacyclic_dft(x: list[int], q: int, psi: int) -> list[int]:
+    """Y[i] = sum_j x[j] psi^((2 brv(i) + 1) j): the definition, O(N^2)."""
+    n = len(x)
+    logn = n.bit_length() - 1
+    out = []
+    for i in range(n):
+        r = pow(psi, 2 * brv(i, logn) + 1, q)
+        acc, p = 0, 1
+        for xj in x:
+            acc = (acc + xj * p) % q
+            p = p * r % q
+        out.append(acc)
+    return out
+
+
+def negacyclic_mul(a: list[int], b: list[int], q: int) -> list[int]:
+    """a * b mod (x^N + 1, q), schoolbook."""
+    n = len(a)
+    c = [0] * n
+    for i, ai in enumerate(a):
+        if ai == 0:
+            continue
+        for j, bj in enumerate(b):
+            k = i + j
+            if k < n:
+                c[k] = (c[k] + ai * bj) % q
+            else:
+                c[k - n] = (c[k - n] - ai * bj) % q
+    return c

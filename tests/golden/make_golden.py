@@ -20,6 +20,12 @@ Writes:
                                      all q-1, all q, ...)
                    blas_<op>_sha     SHA-256 of each BLAS op at 2^16 elements
                    arith_*           add/sub/mul of boundary operand pairs
+                   nc_*              NTT-friendly prime mode: the reference
+                                     ntt() run with q = 2^124 - (62*2^21 - 1),
+                                     mu = floor(2^251/q) and root-power tables
+                                     T[k] = psi^brv(k) (computed here in pure
+                                     Python): nc_y_<logn> (2..12), nc_sha_<logn>
+                                     (13..20), nc_q, nc_root21
 """
 from __future__ import annotations
 
@@ -105,6 +111,18 @@ def main() -> None:
         for op in ("addmod", "submod", "mulmod"):
             gen[f"arith_{op}_{qname}"] = C.to_pairs(
                 [C.ref_scalar(op, x, y, qq, mu) for x, y in zip(pa, pb)])
+    qn = C.ntt_prime_py(C.NC_LOG2_ORDER)
+    mun = (1 << 251) // qn
+    gen["nc_q"] = C.to_pairs([qn])
+    gen["nc_root21"] = C.to_pairs([C.root_of_unity_py(qn, C.NC_LOG2_ORDER)])
+    for logn in range(2, 21):
+        n = 1 << logn
+        x = C.uniform_pairs(SEED_X + logn, n, qn)
+        t = C.negacyclic_table(qn, logn, C.negacyclic_psi(qn, logn))
+        y = C.ref_ntt(x, t, logn, qn, mun, threads=8)
+        if logn <= 12:
+            gen[f"nc_y_{logn}"] = y
+        gen[f"nc_sha_{logn}"] = np.array(sha(y))
     np.savez_compressed(os.path.join(HERE, "ref_gen.npz"), **gen)
     print("wrote", sorted(out), "and", len(gen), "generated fixtures")
 

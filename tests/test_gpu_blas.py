@@ -94,7 +94,8 @@ def test_reference_arith_full_range_random(ctx_ref, op):
 
 
 @pytest.mark.parametrize("op", OPS)
-@pytest.mark.parametrize("q", [(1 << 123) + 12345678901, (1 << 124) - 3, (1 << 100) + 7])
+@pytest.mark.parametrize("q", [(1 << 123) + 12345678901, (1 << 124) - 3, (1 << 124) - 0x7bfffff,
+                               (1 << 124) - ((1 << 31) - 1), (1 << 100) + 7])
 def test_other_moduli_match_oracle(ctx, op, q):
     mu = (1 << 251) // q if q > (1 << 123) else ((1 << 251) // q) & ((1 << 128) - 1)
     n = 5000

@@ -137,7 +137,8 @@ def test_in_place(ctx, logn):
     assert np.array_equal(run_dev(ctx, x, t, logn, inplace=True), C.oracle_ntt(x, t, logn))
 
 
-@pytest.mark.parametrize("q", [(1 << 124) - 3, (1 << 123) + 12345678901, (1 << 127) + 99])
+@pytest.mark.parametrize("q", [(1 << 124) - 3, (1 << 124) - 0x7bfffff, (1 << 124) - ((1 << 31) - 1),
+                               (1 << 123) + 12345678901, (1 << 127) + 99])
 @pytest.mark.parametrize("logn", [4, 10, 12])
 def test_other_moduli(ctx, q, logn):
     mu = ((1 << 251) // q) & ((1 << 128) - 1)

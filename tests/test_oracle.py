@@ -102,7 +102,12 @@ def test_strict_addmod_returns_q():
     assert C.oracle_scalar("addmod", 1, q - 1, q) == q
 
 
-@pytest.mark.parametrize("q,mu", [(C.Q_NTT, C.MU_NTT), (C.Q_BLAS, C.MU_BLAS)])
+_Q_NC = (1 << 124) - (62 * (1 << 21) - 1)      # NTT-friendly prime, 2^21 | q - 1
+_Q_K31 = (1 << 124) - ((1 << 31) - 1)           # largest k the fast path accepts
+
+
+@pytest.mark.parametrize("q,mu", [(C.Q_NTT, C.MU_NTT), (C.Q_BLAS, C.MU_BLAS),
+                                  (_Q_NC, (1 << 251) // _Q_NC), (_Q_K31, (1 << 251) // _Q_K31)])
 def test_reference_barrett_is_exact_on_domain(q, mu):
     """For q = 2^124 - k and mu = floor(2^251/q) the reference quotient is
     within one of the true quotient, so mulmod128 returns a*b mod q exactly for
