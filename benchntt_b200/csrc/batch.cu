@@ -24,7 +24,9 @@ void set_batch_minb(int m) { g_batch_minb = m == 2 ? 2 : 3; }
 size_t shape_smem(int s) {
   const BatchShape& b = kShapes[s];
   const int npass = (b.m + b.logr - 1) / b.logr;
-  return npass > 1 ? (size_t)b.tpc * ((size_t)1 << b.m) * 16 : 0;
+  if (npass <= 1) return 0;
+  if (b.m <= 2) return (size_t)b.tpc * ((size_t)1 << b.m) * 16;  // one-thread tiles
+  return NttEngine<3, ArithFast>::smem_slots(b.m, b.map, kBatchThreads) * 16;
 }
 
 // First shape for (m, map) with the preferred radix (0 = any).

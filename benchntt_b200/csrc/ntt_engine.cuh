@@ -8,10 +8,10 @@
 // at most LOGR stages, passes exchange through XOR-swizzled shared memory --
 // but only the butterfly body of a pass is specialised, on the pass width r.
 // Index arithmetic (which elements a thread owns, where they live) is runtime
-// integer work done once per element per pass, and the register tile is
-// still indexed statically.  One engine covers every size 2^LOGR..2^10 and
-// both thread mappings; its shared memory is threads * R * 16 bytes for all
-// of them.
+// integer work (a group base per pass, then one add per element), and the
+// register tile is still indexed statically.  One engine covers every size
+// 2^LOGR..2^10 and both thread mappings; its shared memory is smem_slots()
+// 16-byte slots.
 #pragma once
 #include "ntt_core.cuh"
 
@@ -47,16 +47,65 @@ struct NttEngine {
     }
   }
 
-  __device__ __forceinline__ static int slot(int M, int map, int tpc, int sub, int idx) {
-    if (map == MAP_INTERLEAVED) return idx * tpc + sub;
-    return (sub << M) | (idx ^ ((idx >> 3) & 7));
+  // Shared-memory slots (16 bytes each) of a tile.  Contiguous tiles give
+  // each sub-transform 2^M + 2^M/8 slots and pad one slot per 8:
+  //   slot = sub * (2^M + 2^M/8) + idx + (idx >> 3)
+  // which spreads the strided accesses of every pass over the banks, and
+  // because idx = base | (j << lo) has disjoint bits, slot(idx) =
+  // slot(base) + pad(j << lo): one add per element once the group's base is
+  // known.  Interleaved tiles use slot = idx * TPC + sub.
+  __host__ __device__ static constexpr size_t smem_slots(int M, int map, int threads) {
+    return map == MAP_INTERLEAVED ? (size_t)threads * R
+                                  : (size_t)(threads >> (M - LOGR)) * (((size_t)1 << M) + ((size_t)1 << M >> 3));
   }
 
-  // r stages on the groups of one pass; register indices are static.
-  template <int r>
-  __device__ __forceinline__ static void body(U128 (&v)[R], const SubRef& sr, int s0, int lo,
-                                              int lane, int tpt, const ModParams& mp) {
+  struct Layout {
+    int contig, tpc, sbase;
+    __device__ __forceinline__ int slot(int idx) const {
+      return contig ? sbase + idx + (idx >> 3) : idx * tpc + sbase;
+    }
+  };
+
+  // One pass of width r (1 <= r <= LOGR) over the thread's GPT = R / 2^r
+  // groups: gather (global on the first pass, else shared), r butterfly
+  // stages with static register indices, scatter (global on the last pass).
+  template <int r, int LDP>
+  __device__ __forceinline__ static void pass(U128 (&v)[R], const SubRef& sr, int s0, int lo,
+                                              int lane, int tpt, bool first, bool last,
+                                              const Layout& lay, uint4* smem, const ModParams& mp,
+                                              int layout) {
     constexpr int G = 1 << r, GPT = R / G;
+    const int hi_mask = ~((1 << lo) - 1);
+    // group i's local index base: (g & lomask) | ((g >> lo) << (lo + r))
+    auto base = [&](int i) {
+      const int g = lane + i * tpt;
+      return g + (g & hi_mask) * (G - 1);
+    };
+    // gather
+#pragma unroll
+    for (int i = 0; i < GPT; ++i) {
+      if (first) {
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+          const int idx = base(i) + (j << lo);
+          if (sr.valid) {
+            v[i * G + j] = from_mem(ld_data<LDP>(sr.x + ((size_t)idx << sr.lshift)), layout);
+          } else {
+#pragma unroll
+            for (int w = 0; w < 4; ++w) v[i * G + j].w[w] = 0u;
+          }
+        }
+      } else {
+        const int sb = lay.slot(base(i));
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+          const int jo = j << lo;
+          const uint4 t = smem[sb + (lay.contig ? jo + (jo >> 3) : jo * lay.tpc)];
+          v[i * G + j] = U128{{t.x, t.y, t.z, t.w}};
+        }
+      }
+    }
+    // r stages per group; stage t of the group reads T[(gt << t) + u], u < 2^t
 #pragma unroll
     for (int i = 0; i < GPT; ++i) {
       const int g = lane + i * tpt;
@@ -76,14 +125,26 @@ struct NttEngine {
         }
       }
     }
-  }
-
-  // Index of element e of the thread's register tile in pass (r, lo).
-  __device__ __forceinline__ static int elem_index(int e, int r, int lo, int lane, int tpt) {
-    const int i = e >> r, j = e & ((1 << r) - 1);
-    const int g = lane + i * tpt;
-    const int base = (g & ((1 << lo) - 1)) | ((g >> lo) << (lo + r));
-    return base | (j << lo);
+    // scatter
+#pragma unroll
+    for (int i = 0; i < GPT; ++i) {
+      if (last) {
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+          const int idx = base(i) + (j << lo);
+          if (sr.valid) sr.y[(size_t)idx << sr.lshift] = to_mem(v[i * G + j], layout);
+        }
+      } else {
+        const int sb = lay.slot(base(i));
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+          const int jo = j << lo;
+          const U128& e = v[i * G + j];
+          smem[sb + (lay.contig ? jo + (jo >> 3) : jo * lay.tpc)] =
+              make_uint4(e.w[0], e.w[1], e.w[2], e.w[3]);
+        }
+      }
+    }
   }
 
   // One tile: `threads` threads, sub-transforms of 2^M points (LOGR <= M <= 10).
@@ -95,45 +156,22 @@ struct NttEngine {
                                              int layout) {
     const Passes ps(M);
     const int tpt = 1 << (M - LOGR);
-    const int tpc = threads >> (M - LOGR);
-    const bool warp_local = map == MAP_CONTIG && tpt <= 32;
+    const bool contig = map == MAP_CONTIG;
+    const bool warp_local = contig && tpt <= 32;
+    Layout lay;
+    lay.contig = contig;
+    lay.tpc = threads >> (M - LOGR);
+    lay.sbase = contig ? sub * ((1 << M) + (1 << M >> 3)) : sub;
     U128 v[R];
     for (int p = 0; p < ps.n; ++p) {
       const int r = ps.bits(p), s0 = ps.start(p), lo = M - s0 - r;
-      // gather
-#pragma unroll
-      for (int e = 0; e < R; ++e) {
-        const int idx = elem_index(e, r, lo, lane, tpt);
-        if (p == 0) {
-          if (sr.valid) {
-            v[e] = from_mem(ld_data<LDP>(sr.x + ((size_t)idx << sr.lshift)), layout);
-          } else {
-#pragma unroll
-            for (int w = 0; w < 4; ++w) v[e].w[w] = 0u;
-          }
-        } else {
-          const uint4 t = smem[slot(M, map, tpc, sub, idx)];
-          v[e] = U128{{t.x, t.y, t.z, t.w}};
-        }
-      }
-      // stages (pass widths run from 2 to LOGR for sizes >= 2^(LOGR+1))
+      const bool first = p == 0, last = p == ps.n - 1;
       if constexpr (LOGR >= 4) {
-        if (r == 4) body<(LOGR >= 4 ? 4 : 1)>(v, sr, s0, lo, lane, tpt, mp);
+        if (r == 4) pass<(LOGR >= 4 ? 4 : 1), LDP>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout);
       }
-      if (r == 3) body<3>(v, sr, s0, lo, lane, tpt, mp);
-      else if (r == 2) body<2>(v, sr, s0, lo, lane, tpt, mp);
-      else if (r == 1) body<1>(v, sr, s0, lo, lane, tpt, mp);
-      // scatter
-      const bool last = p == ps.n - 1;
-#pragma unroll
-      for (int e = 0; e < R; ++e) {
-        const int idx = elem_index(e, r, lo, lane, tpt);
-        if (last) {
-          if (sr.valid) sr.y[(size_t)idx << sr.lshift] = to_mem(v[e], layout);
-        } else {
-          smem[slot(M, map, tpc, sub, idx)] = make_uint4(v[e].w[0], v[e].w[1], v[e].w[2], v[e].w[3]);
-        }
-      }
+      if (r == 3) pass<3, LDP>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout);
+      else if (r == 2) pass<2, LDP>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout);
+      else if (r == 1) pass<1, LDP>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout);
       if (!last) {
         if (warp_local) __syncwarp();
         else __syncthreads();
