@@ -212,10 +212,11 @@ __device__ __noinline__ void run_item_engine(const WorkItem& it, const BatchArgs
   E::place(threadIdx.x, m, map, kBatchThreads, &sub, &lane);
   SubRef sr;
   if (!item_subref(it, ba, m, sub, s_flag, &sr)) return;
-  if (it.kind == ITEM_PASS && it.pass > 0)
-    E::template run<LD_CG>(m, map, kBatchThreads, sr, sub, lane, smem, mp, layout);
-  else
-    E::template run<LD_NC>(m, map, kBatchThreads, sr, sub, lane, smem, mp, layout);
+  // One load policy for every item: L2-coherent loads (a later pass reads what
+  // other CTAs wrote in this launch).  A second instantiation for first
+  // passes would double the engine's code, and instruction fetch is one of
+  // the kernel's main stalls.
+  E::template run<LD_CG>(m, map, kBatchThreads, sr, sub, lane, smem, mp, layout);
   item_publish(it, ba);
 }
 

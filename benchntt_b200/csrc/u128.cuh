@@ -116,6 +116,58 @@ __device__ __forceinline__ U128 submod_ref(const U128& a, const U128& b, const U
   return r;
 }
 
+// The same two operations for q = 2^124 - k with k < 2^31, whose limbs are
+// (2^32 - k, 0xFFFFFFFF, 0xFFFFFFFF, 0x0FFFFFFF): three of them become
+// immediates, which frees registers in the butterfly loops.
+__device__ __forceinline__ U128 addmod_pm(const U128& a, const U128& b, uint32_t q0) {
+  uint32_t s0, s1, s2, s3, e0, e1, e2, e3, gt;
+  asm("add.cc.u32  %0, %9, %13;\n\t"
+      "addc.cc.u32 %1, %10, %14;\n\t"
+      "addc.cc.u32 %2, %11, %15;\n\t"
+      "addc.u32    %3, %12, %16;\n\t"
+      "sub.cc.u32  %4, %17, %0;\n\t"
+      "subc.cc.u32 %5, 0xFFFFFFFF, %1;\n\t"
+      "subc.cc.u32 %6, 0xFFFFFFFF, %2;\n\t"
+      "subc.cc.u32 %7, 0x0FFFFFFF, %3;\n\t"
+      "subc.u32    %8, 0, 0;\n\t"
+      : "=&r"(s0), "=&r"(s1), "=&r"(s2), "=&r"(s3), "=&r"(e0), "=&r"(e1), "=&r"(e2),
+        "=&r"(e3), "=r"(gt)
+      : "r"(a.w[0]), "r"(a.w[1]), "r"(a.w[2]), "r"(a.w[3]), "r"(b.w[0]), "r"(b.w[1]),
+        "r"(b.w[2]), "r"(b.w[3]), "r"(q0));
+  uint32_t n0, n1;
+  asm("sub.cc.u32 %0, 0, %2;\n\t"
+      "subc.u32   %1, 0, %3;\n\t"
+      : "=r"(n0), "=r"(n1)
+      : "r"(e0), "r"(e1));
+  U128 r;
+  const bool sub = gt != 0u;
+  r.w[0] = sub ? n0 : s0;
+  r.w[1] = sub ? n1 : s1;
+  r.w[2] = sub ? ~e2 : s2;
+  r.w[3] = sub ? ~e3 : s3;
+  return r;
+}
+
+__device__ __forceinline__ U128 submod_pm(const U128& a, const U128& b, uint32_t q0) {
+  uint32_t d0, d1, d2, d3, bw;
+  asm("sub.cc.u32  %0, %5, %9;\n\t"
+      "subc.cc.u32 %1, %6, %10;\n\t"
+      "subc.cc.u32 %2, %7, %11;\n\t"
+      "subc.cc.u32 %3, %8, %12;\n\t"
+      "subc.u32    %4, 0, 0;\n\t"
+      : "=&r"(d0), "=&r"(d1), "=&r"(d2), "=&r"(d3), "=r"(bw)
+      : "r"(a.w[0]), "r"(a.w[1]), "r"(a.w[2]), "r"(a.w[3]), "r"(b.w[0]), "r"(b.w[1]),
+        "r"(b.w[2]), "r"(b.w[3]));
+  U128 r;
+  asm("add.cc.u32  %0, %4, %8;\n\t"
+      "addc.cc.u32 %1, %5, %9;\n\t"
+      "addc.cc.u32 %2, %6, %9;\n\t"
+      "addc.u32    %3, %7, %10;\n\t"
+      : "=r"(r.w[0]), "=r"(r.w[1]), "=r"(r.w[2]), "=r"(r.w[3])
+      : "r"(d0), "r"(d1), "r"(d2), "r"(d3), "r"(q0 & bw), "r"(bw), "r"(bw & 0x0FFFFFFFu));
+  return r;
+}
+
 // ------------------------------------------------------------------ ArithFast
 
 // p = a * b, full 256-bit product, operand scanning with two carry chains per
@@ -297,9 +349,15 @@ struct ArithRef {
 template <class Arith>
 __device__ __forceinline__ void butterfly(U128& x, U128& y, const U128& w, const ModParams& m) {
   const U128 p = Arith::mul(w, y, m);
-  const U128 s = addmod_ref(x, p, m.q);
-  y = submod_ref(x, p, m.q);
-  x = s;
+  if constexpr (Arith::kFast) {  // q = 2^124 - k: limbs 1..3 are constants
+    const U128 s = addmod_pm(x, p, m.q.w[0]);
+    y = submod_pm(x, p, m.q.w[0]);
+    x = s;
+  } else {
+    const U128 s = addmod_ref(x, p, m.q);
+    y = submod_ref(x, p, m.q);
+    x = s;
+  }
 }
 
 }  // namespace bntt
