@@ -331,7 +331,10 @@ int bntt_batch_run_host(bntt_batch* b, const bntt_job* jobs, size_t count) {
       total += bytes_of(i);
     }
     if (int rc = grow(c, &b->region, &b->region_cap, total)) return rc;
-    const size_t target = std::max<size_t>(total / 8, 16u << 20);
+    // 16 groups: copies in, kernels and copies out of neighbouring groups
+    // overlap; fewer groups leave longer pipeline fill and drain, more add
+    // launch and event overhead (measured on B200 over PCIe Gen5 x16).
+    const size_t target = std::max<size_t>(total / 16, 8u << 20);
     b->group_first.clear();
     b->group_first.push_back(0);
     size_t acc = 0;
