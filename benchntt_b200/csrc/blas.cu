@@ -4,8 +4,8 @@
 // Each element is 16 bytes; a thread moves U elements per iteration with
 // 128-bit loads marked evict-first (every byte is touched once), so the
 // kernels are bound by HBM bandwidth: 48 bytes per element (two reads, one
-// write).  No shared memory; the grid is a whole number of waves over the
-// SMs and walks the vector with a grid-stride loop.
+// write).  No shared memory; the grid is up to 8 waves of resident blocks
+// and walks the vector with a grid-stride loop.
 #include <algorithm>
 
 #include "internal.h"
@@ -73,8 +73,10 @@ int launch_blas(bntt_ctx* ctx, int op, void* c, const void* a, const void* b, U1
   }
   const size_t per_block = (size_t)kBlasThreads * kBlasUnroll;
   const size_t blocks_needed = (len + per_block - 1) / per_block;
-  // two waves of resident blocks keep enough loads in flight
-  const size_t cap = (size_t)bps_cache[slot] * (size_t)ctx->sms * 2;
+  // up to 8 waves of resident blocks: at 2^24 elements (805 MB per op) a
+  // sweep of unroll x waves on B200 put 8 waves at 103-104 % of the measured
+  // copy bandwidth for vvadd, vvmul and axpy, against 91-99 % at 2 waves
+  const size_t cap = (size_t)bps_cache[slot] * (size_t)ctx->sms * 8;
   const unsigned grid = (unsigned)std::min(blocks_needed, cap);
   uint4* cc = static_cast<uint4*>(c);
   const uint4* aa = static_cast<const uint4*>(a);
