@@ -421,11 +421,40 @@ def e2e_uneven(args, dist, ctx, engine, batch, pid) -> dict:
     dt = (time.perf_counter() - t0) / steps
     dt = dist.max(dt)
     nbytes = batch.total * 16
+    link = pcie_both_ways(xh, yh)
     del xh, yh
     return {"value": batch.count * dist.world / dt, "unit": UNIT, "h2d_bytes_per_step": nbytes,
             "d2h_bytes_per_step": nbytes, "ms_per_step": dt * 1e3, "steps": steps,
             "api": "bntt_batch_run_host (pinned host buffers; pipelined copies)",
-            "pcie_gbs_each_way": nbytes / dt / 1e9}
+            "pcie_gbs_each_way": nbytes / dt / 1e9,
+            "pcie_peak_gbs_each_way": link,
+            "pcie_frac": (nbytes / dt / 1e9) / link if link else None,
+            "pcie_peak_source": "measured live: concurrent pinned H2D and D2H copies of the same buffers"}
+
+
+def pcie_both_ways(xh, yh) -> float:
+    """GB/s each way of plain concurrent pinned copies (H2D of xh, D2H into
+    yh): the link bound of the host path."""
+    import torch
+    dx = torch.empty_like(xh, device="cuda")
+    dy = torch.empty_like(yh, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def both():
+        with torch.cuda.stream(s1):
+            dx.copy_(xh, non_blocking=True)
+        with torch.cuda.stream(s2):
+            yh.copy_(dy, non_blocking=True)
+
+    both()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        both()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / 3
+    del dx, dy
+    return xh.numel() * 8 / dt / 1e9
 
 
 def per_call(args, dist, ctx, stream, engine, jobs, batch, batched_value) -> dict:

@@ -169,9 +169,11 @@ struct NttEngine {
       if constexpr (LOGR >= 4) {
         if (r == 4) pass<(LOGR >= 4 ? 4 : 1), LDP>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout);
       }
+      // with LOGR = 3 the balanced passes of 2^3..2^10 points have 2 or 3
+      // stages, so width 1 needs no code there
       if (r == 3) pass<3, LDP>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout);
       else if (r == 2) pass<2, LDP>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout);
-      else if (r == 1) pass<1, LDP>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout);
+      else if (LOGR != 3) pass<1, LDP>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout);
       if (!last) {
         if (warp_local) __syncwarp();
         else __syncthreads();
