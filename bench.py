@@ -336,6 +336,7 @@ def run_ours(args, dist: Dist):
         "frac": achieved / imad_peak, "peak_source": "measured live: bntt_probe_imad_peak",
         "algorithmic": f"{IMAD_PER_BUTTERFLY} IMAD per butterfly x {bfly} butterflies per launch",
         "traffic": traffic,
+        "butterfly_ceiling": butterfly_ceiling(ctx, bfly, ms_local),
         "hbm": {"achieved_gbs": alg_bytes / (ms_local * 1e-3) / 1e9,
                 "peak_gbs": peaks.get("hbm_gbs"), "algorithmic_bytes": alg_bytes,
                 "frac": (alg_bytes / (ms_local * 1e-3) / 1e9) / peaks["hbm_gbs"]
@@ -385,6 +386,15 @@ def run_ours(args, dist: Dist):
     for p in plans.values():
         p.close()
     return result, ctx
+
+
+def butterfly_ceiling(ctx, bfly: int, ms: float) -> dict:
+    """The kernel's butterfly rate against the same butterfly on registers
+    (no memory, no index arithmetic) at the same occupancy."""
+    peak = ctx.butterfly_peak()
+    achieved = bfly / (ms * 1e-3)
+    return {"achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "G butterflies/s",
+            "frac": achieved / peak, "peak_source": "measured live: bntt_probe_butterfly_peak"}
 
 
 def measured_peaks() -> dict:

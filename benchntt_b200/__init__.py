@@ -139,6 +139,7 @@ _SIGS = [
     ("bntt_batch_inject_wait_timeout", _I, [_P, ctypes.c_uint32]),
     ("bntt_batch_last_launches", _S, [_P]),
     ("bntt_probe_imad_peak", _I, [_P, ctypes.POINTER(ctypes.c_double)]),
+    ("bntt_probe_butterfly_peak", _I, [_P, ctypes.POINTER(ctypes.c_double)]),
     ("bntt_server_create", _I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _S, _PM,
                                 ctypes.POINTER(ServerConfigC)]),
     ("bntt_server_destroy", _I, [_P]),
@@ -298,6 +299,13 @@ class Context:
         """Measured 32-bit IMAD operations per second of this device."""
         v = ctypes.c_double()
         check(lib().bntt_probe_imad_peak(self._h, ctypes.byref(v)))
+        return v.value
+
+    def butterfly_peak(self) -> float:
+        """Measured butterflies per second of the kernels' own butterfly on
+        register-resident data (bntt_probe_butterfly_peak)."""
+        v = ctypes.c_double()
+        check(lib().bntt_probe_butterfly_peak(self._h, ctypes.byref(v)))
         return v.value
 
     def close(self) -> None:

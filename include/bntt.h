@@ -136,7 +136,8 @@ int bntt_plan_destroy(bntt_plan *plan);
 unsigned bntt_plan_log2n(const bntt_plan *plan);
 
 /* NTT-friendly prime mode.  The reference's tables are arbitrary constants
- * (data/twd_N.txt; 2^124 - 719 has no 2-power roots of unity), but ntt()
+ * (data/twd_N.txt; 2^124 - 719 has 2-power roots of unity only up to order
+ * 16), but ntt()
  * takes modulus, mu and table at run time (src/ntt_scalar.c:582), so the same
  * network computes the negacyclic transform
  *     Y[i] = sum_j X[j] * psi^((2*brv(i) + 1) * j)  mod q
@@ -358,6 +359,11 @@ int bntt_autotune_reset(void);
  * roofline the NTT kernels are reported against.  No reference counterpart
  * (the reference times CPU code only, src/ntt_scalar.c:670-683). */
 int bntt_probe_imad_peak(bntt_ctx *ctx, double *ops_per_second);
+/* Butterflies per second of the kernels' own butterfly (fast multiply,
+ * reference add/sub) on register-resident data at the persistent kernel's
+ * occupancy: the compute ceiling of the NTT kernels, with no memory traffic
+ * or index arithmetic. */
+int bntt_probe_butterfly_peak(bntt_ctx *ctx, double *butterflies_per_second);
 
 #ifdef __cplusplus
 }
