@@ -379,6 +379,8 @@ def run_ours(args, dist: Dist):
     result["fused_mul"] = fused_bench(args, ctx, stream)
     # ------------------------------------------- NTT-friendly prime (negacyclic)
     result["negacyclic"] = negacyclic_bench(args, ctx, stream, batch, value)
+    # ------------------------------- inverse transform and polynomial products
+    result["polymul"] = polymul_bench(args, ctx, stream)
     # --------------------------------------------------------------- serving
     engine.close()
     del x, y
@@ -608,6 +610,55 @@ def fused_bench(args, ctx, stream, sizes=(4, 7, 10, 16)) -> dict:
         res[str(n)] = row
         plan.close()
         del x, b, y
+    return res
+
+
+def polymul_bench(args, ctx, stream, sizes=(10, 16)) -> dict:
+    """Negacyclic products a * b mod (x^N + 1) in the friendly-prime mode, 2^26
+    coefficients per operand: forward(b), forward(a) fused with the pointwise
+    product, inverse.  Also the inverse transform alone."""
+    import torch
+
+    import benchntt_b200 as bn
+    L = bn.lib()
+    q, mu = bn.ntt_prime(21)
+    w = bn.root_of_unity(q, mu, 21)
+    mod = bn.modulus(q, mu)
+    total = 1 << 26
+    res = {"modulus": f"2^124 - {(1 << 124) - q:#x}"}
+    for logn in sizes:
+        count = total >> logn
+        plan = bn.Plan.negacyclic(ctx, logn, q, mu, bn.powmod(q, mu, w, 1 << (21 - logn - 1)))
+        a = torch.empty((total, 2), dtype=torch.int64, device=ctx.device)
+        b, bh, c = torch.empty_like(a), torch.empty_like(a), torch.empty_like(a)
+        bn.check(L.bntt_fill_uniform_dev(ctx.handle, a.data_ptr(), total, 21, 0, ctypes.byref(mod), 0))
+        bn.check(L.bntt_fill_uniform_dev(ctx.handle, b.data_ptr(), total, 22, 0, ctypes.byref(mod), 0))
+
+        def product():
+            plan.forward(bh, b, count)
+            plan.forward_mul(c, a, bh, True, count)
+            plan.inverse(c, c, count)
+
+        def inverse_only():
+            plan.inverse(c, bh, count)
+
+        row = {"transforms": count}
+        for name, fn in (("inverse", inverse_only), ("product", product)):
+            for _ in range(3):
+                fn()
+            e0, e1 = cuda_events()
+            reps = max(5, args.steps // 4)
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            row[f"{name}_ms"] = ms
+            row[f"{name}_per_s"] = count / (ms * 1e-3)
+        res[str(1 << logn)] = row
+        plan.close()
+        del a, b, bh, c
     return res
 
 

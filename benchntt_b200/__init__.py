@@ -129,6 +129,7 @@ _SIGS = [
     ("bntt_ntt_forward_dev", _I, [_P, _P, _P, _S]),
     ("bntt_ntt_forward_host", _I, [_P, _P, _P, _S]),
     ("bntt_ntt_forward_mul_dev", _I, [_P, _P, _P, _P, _I, _S]),
+    ("bntt_ntt_inverse_dev", _I, [_P, _P, _P, _S]),
     ("bntt_batch_create", _I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _S]),
     ("bntt_batch_destroy", _I, [_P]),
     ("bntt_batch_run_dev", _I, [_P, ctypes.POINTER(JobC), _S]),
@@ -365,6 +366,12 @@ class Plan:
         else:
             b = batch if batch is not None else x.size // (2 * n)
             check(lib().bntt_ntt_forward_host(self._h, _host_ptr(y), _host_ptr(x), b))
+
+    def inverse(self, x, y, batch: int | None = None) -> None:
+        """x = ntt^-1(y) (bntt_ntt_inverse_dev); device tensors only."""
+        n = 1 << self.log2n
+        bt = batch if batch is not None else y.numel() // (2 * n)
+        check(lib().bntt_ntt_inverse_dev(self._h, _dev_ptr(x), _dev_ptr(y), bt))
 
     def forward_mul(self, y, x, b, per_transform: bool = True, batch: int | None = None) -> None:
         """y = ntt(x) o b in one launch sequence (bntt_ntt_forward_mul_dev);

@@ -46,6 +46,9 @@ u128 barrett_mu(u128 q);
 // True when the pseudo-Mersenne multiply is bit-identical to the reference.
 bool modulus_fast(u128 q, u128 mu, uint32_t* k_out);
 ModParams make_params(const bntt_modulus& m, bool* fast_out);
+// Exact host arithmetic for 2^123 < q < 2^124, mu = floor(2^251 / q); a, b < q.
+u128 host_mulmod(u128 a, u128 b, u128 q, u128 mu);
+u128 host_powmod(u128 a, u128 e, u128 q, u128 mu);
 
 // ----------------------------------------------------------------- kernels
 struct SubGeom;  // ntt_core.cuh
@@ -117,6 +120,10 @@ struct bntt_plan {
   int layout = 0;
   void* tw = nullptr;
   bool own_tw = false;
+  // inverse transform: table of inverse twiddles (limb order) and N^-1 mod q,
+  // built on the first inverse call
+  void* tw_inv = nullptr;
+  bntt::U128 ninv{};
   // kernel per HBM pass
   std::vector<int> passes;
   std::vector<const bntt::SubKernel*> kernels;

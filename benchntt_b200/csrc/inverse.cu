@@ -1,0 +1,186 @@
+// inverse.cu -- inverse of the plan's forward transform.
+//
+// The reference has no inverse transform.  The forward network
+// (src/ntt_scalar.c:582-627, in its in-place form: stage s pairs indices
+// that differ in bit n-1-s with twiddle T[2^s + (index >> (n-s))]) is a
+// product of butterflies (x, y) -> (x + w y, x - w y); each is invertible
+// when w is, with inverse (u, v) -> ((u + v) / 2, (u - v) / (2 w)).  So
+// running the stages from the last to the first with Gentleman-Sande
+// butterflies (x, y) -> (x + y, (x - y) w^-1) and multiplying by N^-1 at the
+// end returns the input, for every table whose entries are invertible mod a
+// prime q.  With the root-power tables of roots.cu it is the inverse
+// negacyclic NTT, and ntt^-1(ntt(a) o ntt(b)) = a * b mod (x^N + 1).
+//
+// Sums here are exact mod q (no reference quirk applies: the reference has
+// no such code); results are canonical residues in [0, q).  The fast
+// pseudo-Mersenne multiply is required (q = 2^124 - k, k < 2^31).
+//
+// Kernels: the runtime-size tile engine (ntt_engine.cuh) in inverse mode,
+// one launch per HBM pass in reverse pass order (the pass over the low index
+// bits first), and a one-thread-per-transform kernel for N = 2 and 4.
+#include <algorithm>
+#include <vector>
+
+#include "internal.h"
+#include "ntt_core.cuh"
+#include "ntt_engine.cuh"
+
+namespace bntt {
+namespace {
+
+constexpr int kInvThreads = 256;
+// Largest HBM pass: a strided pass of 2^m points then covers
+// 256 >> (m - 3) >= 8 adjacent columns (128 contiguous bytes per row).
+constexpr int kInvMaxPass = 8;
+
+using InvEngine = NttEngine<3, ArithFast>;
+
+__global__ void __launch_bounds__(kInvThreads, 3)
+    k_ntt_inv(SubGeom g, ModParams mp, int layout, int m, int map, U128 scale, int do_scale) {
+  extern __shared__ uint4 smem[];
+  int sub, lane;
+  InvEngine::place(threadIdx.x, m, map, kInvThreads, &sub, &lane);
+  const int tpc = kInvThreads >> (m - 3);
+  const uint64_t ntiles = (g.nsub + (uint64_t)tpc - 1) / (uint64_t)tpc;
+  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const SubRef sr = make_subref(g, tile * (uint64_t)tpc + (uint64_t)sub);
+    InvEngine::run<LD_CG, true>(m, map, kInvThreads, sr, sub, lane, smem, mp, layout,
+                                do_scale ? &scale : nullptr);
+    __syncthreads();  // shared memory is reused by the next tile
+  }
+}
+
+// N = 2 or 4: one thread per transform, stages in reverse order, then N^-1.
+__global__ void __launch_bounds__(256)
+    k_ntt_inv_tiny(uint4* x, const uint4* y, const uint4* tw, uint64_t count, int n, ModParams mp,
+                   int layout, U128 scale) {
+  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const int N = 1 << n;
+  U128 v[4];
+  for (int i = 0; i < N; ++i) v[i] = from_mem(__ldcg(y + t * N + i), layout);
+  for (int s = n - 1; s >= 0; --s) {
+    const int half = N >> (s + 1);
+    for (int i = 0; i < N; ++i) {
+      if (i & half) continue;
+      const uint4 tv = __ldg(tw + (1 << s) + (i >> (n - s)));
+      gs_butterfly<ArithFast>(v[i], v[i + half], U128{{tv.x, tv.y, tv.z, tv.w}}, mp);
+    }
+  }
+  for (int i = 0; i < N; ++i) x[t * N + i] = to_mem(ArithFast::mul(v[i], scale, mp), layout);
+}
+
+int inv_blocks_per_sm(size_t smem) {
+  static int cached[2] = {0, 0};
+  const int slot = smem > 0 ? 1 : 0;
+  if (cached[slot]) return cached[slot];
+  int b = 0;
+  BNTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void*)k_ntt_inv, kInvThreads,
+                                                        smem));
+  cached[slot] = std::max(1, b);
+  return cached[slot];
+}
+
+// Inverse table (T[k]^-1, limb order) and N^-1, built once per plan: the
+// forward table comes back from the device and is inverted on the host with
+// one modular exponentiation and three multiplies per entry (batch
+// inversion).
+int ensure_inverse(bntt_plan* p) {
+  if (p->tw_inv) return BNTT_OK;
+  const u128 q = to_u128(p->mod.q), mu = to_u128(p->mod.mu);
+  const size_t n = (size_t)1 << p->log2n;
+  std::vector<uint32_t> t(4 * n);
+  BNTT_CK(cudaMemcpy(t.data(), p->tw, n * 16, cudaMemcpyDeviceToHost));
+  auto entry = [&](size_t k) {
+    u128 v = 0;
+    for (int l = 3; l >= 0; --l) v = (v << 32) | t[4 * k + l];
+    return v;
+  };
+  // prefix products, one inverse, then walk back
+  std::vector<u128> pre(n, 1);
+  u128 acc = 1;
+  for (size_t k = 1; k < n; ++k) {
+    const u128 e = entry(k);
+    BNTT_REQUIRE(e != 0 && e < q, "twiddle %zu is 0 mod q (or not a residue): no inverse", k);
+    pre[k] = acc;
+    acc = host_mulmod(acc, e, q, mu);
+  }
+  u128 inv = host_powmod(acc, q - 2, q, mu);
+  BNTT_REQUIRE(host_mulmod(inv, acc, q, mu) == 1,
+               "the product of the twiddles has no inverse mod q (q is not prime)");
+  std::vector<uint32_t> ti(4 * n, 0);
+  ti[0] = 1;  // entry 0 is never read
+  for (size_t k = n - 1; k >= 1; --k) {
+    const u128 ik = host_mulmod(inv, pre[k], q, mu);  // = T[k]^-1
+    inv = host_mulmod(inv, entry(k), q, mu);
+    for (int l = 0; l < 4; ++l) ti[4 * k + l] = (uint32_t)(ik >> (32 * l));
+  }
+  const u128 ninv = host_powmod((u128)n % q, q - 2, q, mu);
+  BNTT_REQUIRE(host_mulmod(ninv, (u128)n % q, q, mu) == 1, "N has no inverse mod q");
+  void* d = nullptr;
+  if (int rc = ctx_alloc(p->ctx, &d, n * 16)) return rc;
+  cudaError_t e = cudaMemcpy(d, ti.data(), n * 16, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    ctx_free(p->ctx, d);
+    return cuda_error(e, "cudaMemcpy(inverse twiddles)");
+  }
+  p->tw_inv = d;
+  p->ninv = to_limbs(ninv);
+  return BNTT_OK;
+}
+
+int inverse_on(bntt_plan* p, void* x, const void* y, size_t batch, cudaStream_t s) {
+  const int n = (int)p->log2n;
+  uint4* xo = static_cast<uint4*>(x);
+  const uint4* yi = static_cast<const uint4*>(y);
+  const uint4* tw = static_cast<const uint4*>(p->tw_inv);
+  if (n <= 2) {
+    const unsigned grid = (unsigned)((batch + 255) / 256);
+    k_ntt_inv_tiny<<<grid, 256, 0, s>>>(xo, yi, tw, (uint64_t)batch, n, p->mp, p->layout, p->ninv);
+    BNTT_CK(cudaGetLastError());
+    p->ctx->launches++;
+    return BNTT_OK;
+  }
+  const std::vector<int> passes = n <= 10 ? std::vector<int>{n} : split_passes(n, kInvMaxPass);
+  std::vector<int> starts(passes.size(), 0);
+  for (size_t i = 1; i < passes.size(); ++i) starts[i] = starts[i - 1] + passes[i - 1];
+  for (int i = (int)passes.size() - 1; i >= 0; --i) {
+    const int m = passes[i];
+    SubGeom g;
+    g.x = i == (int)passes.size() - 1 ? yi : xo;  // first executed pass reads the input
+    g.y = xo;
+    g.tw = tw;
+    g.n = (uint32_t)n;
+    g.s0 = (uint32_t)starts[i];
+    g.m = (uint32_t)m;
+    g.l = (uint32_t)(n - starts[i] - m);
+    g.nsub = (uint64_t)batch << (n - m);
+    const int map = g.l > 0 ? MAP_INTERLEAVED : MAP_CONTIG;
+    const size_t smem = InvEngine::smem_slots(m, map, kInvThreads) * 16;
+    const int bps = inv_blocks_per_sm(smem);
+    const int tpc = kInvThreads >> (m - 3);
+    const uint64_t ntiles = (g.nsub + (uint64_t)tpc - 1) / (uint64_t)tpc;
+    const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)bps * p->ctx->sms);
+    k_ntt_inv<<<grid, kInvThreads, smem, s>>>(g, p->mp, p->layout, m, map, p->ninv, i == 0 ? 1 : 0);
+    BNTT_CK(cudaGetLastError());
+    p->ctx->launches++;
+  }
+  return BNTT_OK;
+}
+
+}  // namespace
+}  // namespace bntt
+
+using namespace bntt;
+
+extern "C" int bntt_ntt_inverse_dev(bntt_plan* p, void* x, const void* y, size_t batch) {
+  BNTT_REQUIRE(p, "plan is NULL");
+  if (batch == 0) return BNTT_OK;
+  BNTT_REQUIRE(x && y, "NULL buffer");
+  BNTT_REQUIRE(((uintptr_t)x & 15) == 0 && ((uintptr_t)y & 15) == 0,
+               "device buffers must be 16-byte aligned");
+  BNTT_REQUIRE(p->fast, "the inverse transform needs q = 2^124 - k (k < 2^31), mu = floor(2^251/q)");
+  if (int rc = ctx_use_device(p->ctx)) return rc;
+  if (int rc = ensure_inverse(p)) return rc;
+  return inverse_on(p, x, y, batch, p->ctx->stream);
+}

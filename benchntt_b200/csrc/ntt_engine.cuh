@@ -69,11 +69,15 @@ struct NttEngine {
   // One pass of width r (1 <= r <= LOGR) over the thread's GPT = R / 2^r
   // groups: gather (global on the first pass, else shared), r butterfly
   // stages with static register indices, scatter (global on the last pass).
-  template <int r, int LDP>
+  //
+  // INV runs the inverse of the same r stages: the stages in reverse order,
+  // each an inverse (Gentleman-Sande) butterfly with the table holding the
+  // inverse twiddles, and on the last store an optional multiply by *scale.
+  template <int r, int LDP, bool INV = false>
   __device__ __forceinline__ static void pass(U128 (&v)[R], const SubRef& sr, int s0, int lo,
                                               int lane, int tpt, bool first, bool last,
                                               const Layout& lay, uint4* smem, const ModParams& mp,
-                                              int layout) {
+                                              int layout, const U128* scale = nullptr) {
     constexpr int G = 1 << r, GPT = R / G;
     const int hi_mask = ~((1 << lo) - 1);
     // group i's local index base: (g & lomask) | ((g >> lo) << (lo + r))
@@ -111,7 +115,8 @@ struct NttEngine {
       const int g = lane + i * tpt;
       const uint32_t gt = (sr.trow << s0) + (uint32_t)(g >> lo);
 #pragma unroll
-      for (int t = 0; t < r; ++t) {
+      for (int tt = 0; tt < r; ++tt) {
+        const int t = INV ? r - 1 - tt : tt;
         const int half = 1 << (r - 1 - t);
 #pragma unroll
         for (int u = 0; u < (1 << t); ++u) {
@@ -120,7 +125,8 @@ struct NttEngine {
 #pragma unroll
           for (int k = 0; k < half; ++k) {
             const int j = (u << (r - t)) | k;
-            butterfly<Arith>(v[i * G + j], v[i * G + j + half], w, mp);
+            if constexpr (INV) gs_butterfly<Arith>(v[i * G + j], v[i * G + j + half], w, mp);
+            else butterfly<Arith>(v[i * G + j], v[i * G + j + half], w, mp);
           }
         }
       }
@@ -132,7 +138,12 @@ struct NttEngine {
 #pragma unroll
         for (int j = 0; j < G; ++j) {
           const int idx = base(i) + (j << lo);
-          if (sr.valid) sr.y[(size_t)idx << sr.lshift] = to_mem(v[i * G + j], layout);
+          if (sr.valid) {
+            if constexpr (INV) {
+              if (scale) v[i * G + j] = Arith::mul(v[i * G + j], *scale, mp);
+            }
+            sr.y[(size_t)idx << sr.lshift] = to_mem(v[i * G + j], layout);
+          }
         }
       } else {
         const int sb = lay.slot(base(i));
@@ -150,10 +161,13 @@ struct NttEngine {
   // One tile: `threads` threads, sub-transforms of 2^M points (LOGR <= M <= 10).
   // Every thread of the CTA calls it; threads of invalid sub-transforms
   // compute on zeros and store nothing.
-  template <int LDP>
+  //
+  // INV = true runs the inverse network of the same passes (last pass first)
+  // and multiplies the stored results by *scale when scale is not null.
+  template <int LDP, bool INV = false>
   __device__ __forceinline__ static void run(int M, int map, int threads, const SubRef& sr,
                                              int sub, int lane, uint4* smem, const ModParams& mp,
-                                             int layout) {
+                                             int layout, const U128* scale = nullptr) {
     const Passes ps(M);
     const int tpt = 1 << (M - LOGR);
     const bool contig = map == MAP_CONTIG;
@@ -163,17 +177,23 @@ struct NttEngine {
     lay.tpc = threads >> (M - LOGR);
     lay.sbase = contig ? sub * ((1 << M) + (1 << M >> 3)) : sub;
     U128 v[R];
-    for (int p = 0; p < ps.n; ++p) {
+    for (int pp = 0; pp < ps.n; ++pp) {
+      const int p = INV ? ps.n - 1 - pp : pp;
       const int r = ps.bits(p), s0 = ps.start(p), lo = M - s0 - r;
-      const bool first = p == 0, last = p == ps.n - 1;
+      const bool first = pp == 0, last = pp == ps.n - 1;
       if constexpr (LOGR >= 4) {
-        if (r == 4) pass<(LOGR >= 4 ? 4 : 1), LDP>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout);
+        if (r == 4)
+          pass<(LOGR >= 4 ? 4 : 1), LDP, INV>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp,
+                                              layout, scale);
       }
       // with LOGR = 3 the balanced passes of 2^3..2^10 points have 2 or 3
       // stages, so width 1 needs no code there
-      if (r == 3) pass<3, LDP>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout);
-      else if (r == 2) pass<2, LDP>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout);
-      else if (LOGR != 3) pass<1, LDP>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout);
+      if (r == 3)
+        pass<3, LDP, INV>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout, scale);
+      else if (r == 2)
+        pass<2, LDP, INV>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout, scale);
+      else if (LOGR != 3)
+        pass<1, LDP, INV>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout, scale);
       if (!last) {
         if (warp_local) __syncwarp();
         else __syncthreads();

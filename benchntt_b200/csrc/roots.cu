@@ -29,8 +29,8 @@
 #include "internal.h"
 
 namespace bntt {
-namespace {
 
+namespace {
 struct U256 {
   u128 hi, lo;
 };
@@ -46,12 +46,13 @@ U256 mul_full(u128 a, u128 b) {
   r.hi = p11 + (p01 >> 64) + (p10 >> 64) + (mid >> 64);
   return r;
 }
+}  // namespace
 
 // a * b mod q for a, b < q, 2^123 < q < 2^124, mu = floor(2^251 / q).
 // P < 2^248; qq = floor(floor(P / 2^122) * mu / 2^129) is floor(P/q) or one
 // less (the truncations lose < 2^122/q + P/2^251 < 5/8), and P - qq*q < 2q
 // fits 128 bits, so it is formed mod 2^128.
-u128 mulmod_exact(u128 a, u128 b, u128 q, u128 mu) {
+u128 host_mulmod(u128 a, u128 b, u128 q, u128 mu) {
   const U256 P = mul_full(a, b);
   const u128 ql = (P.hi << 6) | (P.lo >> 122);
   const U256 t = mul_full(ql, mu);
@@ -61,15 +62,17 @@ u128 mulmod_exact(u128 a, u128 b, u128 q, u128 mu) {
   return r;
 }
 
-u128 powmod(u128 a, u128 e, u128 q, u128 mu) {
+u128 host_powmod(u128 a, u128 e, u128 q, u128 mu) {
   u128 r = 1, b = a % q;
   while (e) {
-    if (e & 1) r = mulmod_exact(r, b, q, mu);
-    b = mulmod_exact(b, b, q, mu);
+    if (e & 1) r = host_mulmod(r, b, q, mu);
+    b = host_mulmod(b, b, q, mu);
     e >>= 1;
   }
   return r;
 }
+
+namespace {
 
 // Strong probable-prime test to the first 24 prime bases.  A composite passes
 // one base with probability at most 1/4, so all 24 with at most 2^-48 in the
@@ -86,11 +89,11 @@ bool miller_rabin(u128 n, u128 mu) {
     ++s;
   }
   for (uint32_t a : kBases) {
-    u128 x = powmod(a, d, n, mu);
+    u128 x = host_powmod(a, d, n, mu);
     if (x == 1 || x == n - 1) continue;
     bool witness = true;
     for (int i = 1; i < s && witness; ++i) {
-      x = mulmod_exact(x, x, n, mu);
+      x = host_mulmod(x, x, n, mu);
       if (x == n - 1) witness = false;
     }
     if (witness) return false;
@@ -163,7 +166,7 @@ int bntt_powmod(const bntt_modulus* m, bntt_u128 a, bntt_u128 e, bntt_u128* out)
   BNTT_REQUIRE(m && out, "NULL argument");
   const u128 q = to_u128(m->q), mu = to_u128(m->mu);
   BNTT_REQUIRE(modulus_in_range(q, mu), "modulus must satisfy 2^123 < q < 2^124, mu = floor(2^251/q)");
-  *out = from_u128(powmod(to_u128(a), to_u128(e), q, mu));
+  *out = from_u128(host_powmod(to_u128(a), to_u128(e), q, mu));
   return BNTT_OK;
 }
 
@@ -178,8 +181,8 @@ int bntt_root_of_unity(const bntt_modulus* m, unsigned log2_order, bntt_u128* ro
   // w = g^((q-1)/2^t) has order dividing 2^t; it is exactly 2^t when
   // w^(2^(t-1)) = -1.  For prime q half of all g give such a w.
   for (uint32_t g = 2; g < 4096; ++g) {
-    const u128 w = powmod(g, cofactor, q, mu);
-    const u128 h = powmod(w, (u128)1 << (log2_order - 1), q, mu);
+    const u128 w = host_powmod(g, cofactor, q, mu);
+    const u128 h = host_powmod(w, (u128)1 << (log2_order - 1), q, mu);
     if (h == q - 1) {
       *root = from_u128(w);
       return BNTT_OK;
@@ -195,12 +198,12 @@ int bntt_twiddles_negacyclic(const bntt_modulus* m, unsigned log2n, bntt_u128 ps
   BNTT_REQUIRE(layout == BNTT_LAYOUT_HILO || layout == BNTT_LAYOUT_U128, "bad layout %d", layout);
   const u128 q = to_u128(m->q), mu = to_u128(m->mu), p = to_u128(psi);
   BNTT_REQUIRE(modulus_in_range(q, mu), "modulus must satisfy 2^123 < q < 2^124, mu = floor(2^251/q)");
-  BNTT_REQUIRE(p < q && powmod(p, (u128)1 << log2n, q, mu) == q - 1,
+  BNTT_REQUIRE(p < q && host_powmod(p, (u128)1 << log2n, q, mu) == q - 1,
                "psi is not a primitive 2^%u-th root of unity (psi^N != -1)", log2n + 1);
   const uint32_t n = 1u << log2n;
   std::vector<u128> pw(n);
   pw[0] = 1;
-  for (uint32_t j = 1; j < n; ++j) pw[j] = mulmod_exact(pw[j - 1], p, q, mu);
+  for (uint32_t j = 1; j < n; ++j) pw[j] = host_mulmod(pw[j - 1], p, q, mu);
   uint64_t* out = static_cast<uint64_t*>(table);
   for (uint32_t k = 0; k < n; ++k) {
     const u128 v = pw[bit_reverse(k, log2n)];
@@ -219,7 +222,7 @@ int bntt_plan_create_negacyclic(bntt_ctx* c, bntt_plan** out, unsigned log2n, co
                "root-power tables are built on the device for q = 2^124 - k (k < 2^31), "
                "mu = floor(2^251/q); build others with bntt_twiddles_negacyclic");
   BNTT_REQUIRE(log2n >= 1 && log2n <= 24, "log2n %u outside [1, 24]", log2n);
-  BNTT_REQUIRE(p < q && powmod(p, (u128)1 << log2n, q, mu) == q - 1,
+  BNTT_REQUIRE(p < q && host_powmod(p, (u128)1 << log2n, q, mu) == q - 1,
                "psi is not a primitive 2^%u-th root of unity (psi^N != -1)", log2n + 1);
   int rc = plan_create_common(c, out, log2n, m, layout);
   if (rc) return rc;
@@ -236,7 +239,7 @@ int bntt_plan_create_negacyclic(bntt_ctx* c, bntt_plan** out, unsigned log2n, co
   for (unsigned i = 0; i < log2n; ++i) {
     const U128 l = to_limbs(f);
     pw.p[i] = make_uint4(l.w[0], l.w[1], l.w[2], l.w[3]);
-    f = mulmod_exact(f, f, q, mu);
+    f = host_mulmod(f, f, q, mu);
   }
   const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)c->sms * 8);
   k_negacyclic_table<<<grid, 256, 0, c->stream>>>(static_cast<uint4*>(pl->tw), log2n, pw, pl->mp);

@@ -454,6 +454,10 @@ int bntt_plan_destroy(bntt_plan* p) {
     ctx_use_device(p->ctx);
     ctx_free(p->ctx, p->tw);
   }
+  if (p->tw_inv) {
+    ctx_use_device(p->ctx);
+    ctx_free(p->ctx, p->tw_inv);
+  }
   delete p;
   return BNTT_OK;
 }

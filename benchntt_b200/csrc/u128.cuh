@@ -360,4 +360,37 @@ __device__ __forceinline__ void butterfly(U128& x, U128& y, const U128& w, const
   }
 }
 
+// Exact a + b mod q for q = 2^124 - k (a, b <= q): the sum less q when it
+// is at least q.  Used by the inverse transform, which has no reference
+// counterpart and computes canonical residues.
+__device__ __forceinline__ U128 addmod_exact_pm(const U128& a, const U128& b, uint32_t q0) {
+  uint32_t s0, s1, s2, s3, t0, t1, t2, t3, bw;
+  asm("add.cc.u32  %0, %9, %13;\n\t"
+      "addc.cc.u32 %1, %10, %14;\n\t"
+      "addc.cc.u32 %2, %11, %15;\n\t"
+      "addc.u32    %3, %12, %16;\n\t"
+      "sub.cc.u32  %4, %0, %17;\n\t"
+      "subc.cc.u32 %5, %1, 0xFFFFFFFF;\n\t"
+      "subc.cc.u32 %6, %2, 0xFFFFFFFF;\n\t"
+      "subc.cc.u32 %7, %3, 0x0FFFFFFF;\n\t"
+      "subc.u32    %8, 0, 0;\n\t"
+      : "=&r"(s0), "=&r"(s1), "=&r"(s2), "=&r"(s3), "=&r"(t0), "=&r"(t1), "=&r"(t2),
+        "=&r"(t3), "=r"(bw)
+      : "r"(a.w[0]), "r"(a.w[1]), "r"(a.w[2]), "r"(a.w[3]), "r"(b.w[0]), "r"(b.w[1]),
+        "r"(b.w[2]), "r"(b.w[3]), "r"(q0));
+  const bool keep = bw != 0u;  // s < q
+  return U128{{keep ? s0 : t0, keep ? s1 : t1, keep ? s2 : t2, keep ? s3 : t3}};
+}
+
+// Inverse (Gentleman-Sande) butterfly: (x, y) <- (x + y, (x - y) * w) with
+// exact sums.  With w the inverse of the forward twiddle it undoes
+// butterfly() up to a factor 2 on both outputs.  Fast moduli only.
+template <class Arith>
+__device__ __forceinline__ void gs_butterfly(U128& x, U128& y, const U128& w, const ModParams& m) {
+  static_assert(Arith::kFast, "the inverse transform uses the pseudo-Mersenne arithmetic");
+  const U128 d = submod_pm(x, y, m.q.w[0]);
+  x = addmod_exact_pm(x, y, m.q.w[0]);
+  y = Arith::mul(w, d, m);
+}
+
 }  // namespace bntt

@@ -170,6 +170,18 @@ int bntt_ntt_forward_dev(bntt_plan *plan, void *y, const void *x, size_t batch);
 /* Host-pointer form: copies in, transforms, copies out (the reference's
  * call shape; pipelined over chunks of the batch). */
 int bntt_ntt_forward_host(bntt_plan *plan, void *y, const void *x, size_t batch);
+/* Inverse of the plan's forward transform: x = ntt^-1(y) for `batch`
+ * contiguous vectors (x may equal y).  The reference has no inverse; this
+ * one runs the forward network's stages in reverse order with inverse
+ * (Gentleman-Sande) butterflies and the inverted table, then multiplies by
+ * N^-1, so ntt^-1(ntt(x)) = x for every table whose entries are invertible
+ * mod a prime q.  With a negacyclic plan it is the inverse negacyclic NTT.
+ * Results are canonical residues in [0, q).  Needs the fast multiply
+ * (q = 2^124 - k, k < 2^31, mu = floor(2^251/q)); the inverse table is
+ * built on the first call (EINVAL if a twiddle is 0 mod q or q is not
+ * prime). */
+int bntt_ntt_inverse_dev(bntt_plan *plan, void *x, const void *y, size_t batch);
+
 /* Transform fused with the pointwise product that follows it in a
  * polynomial-multiply pipeline:  y_t = vector_mul(ntt(x_t), b_t)
  * (src/ntt_scalar.c:582 then src/blas_scalar.c:594) under the plan's

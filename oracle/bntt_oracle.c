@@ -14,6 +14,8 @@
  *   mulmod128   src/ntt_scalar.c:173-199  (Barrett, MBITS = 124)
  *   ntt         src/ntt_scalar.c:582-627  (constant-geometry radix-2 network)
  *   vector_add / vector_sub / vector_mul / axpy   src/blas_scalar.c:578-608
+ * and, with no reference counterpart, the inverse of the network
+ * (orc_ntt_inverse_batch), the checker of libbntt's inverse transform.
  *
  * Every 64-bit word operation keeps the reference's truncation points, so the
  * results equal the reference's for ANY 128-bit inputs, including the two
@@ -25,7 +27,7 @@
  * Parity pin: tests/test_oracle.py checks this file against the reference's
  * golden vectors (data/ver_N.txt, data/{vvadd,vvsub,vvmul,axpy}_1024.txt,
  * committed as tests/golden/ref_data.npz) and against the reference compiled
- * from its own sources (oracle/_ref, built by oracle/build_ref.sh).
+ * from its own sources (oracle/_ref, built by `make -C oracle ref`).
  *
  * Buffers at the C ABI are "hi-first u64 pairs": element i is buf[2i] (high
  * 64 bits) and buf[2i+1] (low 64 bits), the layout of the reference's data
@@ -294,6 +296,74 @@ void orc_ntt_batch(uint64_t *Y, const uint64_t *X, const uint64_t *T, int logn, 
     }
     orc_ntt_jobs(ys, xs, ts, ls, batch, mh, ml, muh, mul, form, threads);
     free(ys); free(xs); free(ts); free(ls);
+}
+
+/* ------------------------------------------------------------ inverse NTT */
+
+/* Not in the reference (it has no inverse transform): the inverse of the
+ * in-place network above, which libbntt's bntt_ntt_inverse_dev computes.
+ * Stages run from logn-1 down to 0; stage s pairs indices that differ in bit
+ * logn-1-s, block b uses Tinv[2^s + b] = T[2^s + b]^-1, and each pair
+ * (x, y) becomes (x + y, (x - y) * w) with exact sums: x + y less q when it
+ * is at least q, x - y plus q on borrow.  Finally every element is
+ * multiplied by N^-1.  Products use orc_mulmod, exact for q = 2^124 - k with
+ * k < 2^31 and mu = floor(2^251/q) (checked by tests/test_oracle.py). */
+static u128 orc_powmod(u128 a, u128 e, u128 m, u128 mu)
+{
+    u128 r = 1;
+    while (e) {
+        if (e & 1) r = orc_mulmod(r, a, m, mu);
+        a = orc_mulmod(a, a, m, mu);
+        e >>= 1;
+    }
+    return r;
+}
+
+static void ntt_inverse_one(u128 *v, int logn, u128 m, u128 mu, const u128 *Tinv, u128 ninv)
+{
+    size_t n = (size_t)1 << logn;
+    for (int s = logn - 1; s >= 0; --s) {
+        size_t half = n >> (s + 1);
+        for (size_t blk = 0; blk < ((size_t)1 << s); ++blk) {
+            u128 w = Tinv[((size_t)1 << s) + blk];
+            size_t base = blk * 2 * half;
+            for (size_t k = base; k < base + half; ++k) {
+                u128 a = v[k], b = v[k + half];
+                u128 sum = a + b;
+                v[k] = sum >= m ? sum - m : sum;
+                v[k + half] = orc_mulmod(w, orc_submod(a, b, m), m, mu);
+            }
+        }
+    }
+    for (size_t i = 0; i < n; ++i) v[i] = orc_mulmod(v[i], ninv, m, mu);
+}
+
+/* `batch` contiguous inverse transforms of size 2^logn; T is the FORWARD
+ * table (2^logn hi-first pairs), inverted here entry by entry (Fermat).
+ * Returns 0, or -1 when an entry or N has no inverse. */
+int orc_ntt_inverse_batch(uint64_t *X, const uint64_t *Y, const uint64_t *T, int logn, size_t batch,
+                          uint64_t mh, uint64_t ml, uint64_t muh, uint64_t mul)
+{
+    u128 m = MK(mh, ml), mu = MK(muh, mul);
+    size_t n = (size_t)1 << logn;
+    u128 *tinv = malloc(n * sizeof(u128)), *v = malloc(n * sizeof(u128));
+    int rc = 0;
+    tinv[0] = 1;
+    for (size_t k = 1; k < n && !rc; ++k) {
+        u128 t = get_pair(T, k);
+        tinv[k] = orc_powmod(t, m - 2, m, mu);
+        if (orc_mulmod(tinv[k], t, m, mu) != 1) rc = -1;
+    }
+    u128 ninv = orc_powmod((u128)n % m, m - 2, m, mu);
+    if (orc_mulmod(ninv, (u128)n % m, m, mu) != 1) rc = -1;
+    for (size_t b = 0; b < batch && !rc; ++b) {
+        for (size_t i = 0; i < n; ++i) v[i] = get_pair(Y, b * n + i);
+        ntt_inverse_one(v, logn, m, mu, tinv, ninv);
+        for (size_t i = 0; i < n; ++i) put_pair(X, b * n + i, v[i]);
+    }
+    free(tinv);
+    free(v);
+    return rc;
 }
 
 /* --------------------------------------------------------------------- BLAS */

@@ -123,6 +123,9 @@ def oracle():
                                       u64, u64, u64, u64, ctypes.c_int, ctypes.c_int]
         lib.orc_ntt_jobs.argtypes = [p, p, p, p, ctypes.c_size_t,
                                      u64, u64, u64, u64, ctypes.c_int, ctypes.c_int]
+        lib.orc_ntt_inverse_batch.argtypes = [p, p, p, ctypes.c_int, ctypes.c_size_t,
+                                              u64, u64, u64, u64]
+        lib.orc_ntt_inverse_batch.restype = ctypes.c_int
         lib.orc_vvadd.argtypes = [p, p, p, ctypes.c_size_t, u64, u64]
         lib.orc_vvsub.argtypes = [p, p, p, ctypes.c_size_t, u64, u64]
         lib.orc_vvmul.argtypes = [p, p, p, ctypes.c_size_t, u64, u64, u64, u64]
@@ -156,6 +159,22 @@ def oracle_ntt(x: np.ndarray, t: np.ndarray, logn: int, q: int = Q_NTT, mu: int 
     lib.orc_ntt_batch(_ptr(y), _ptr(x), _ptr(t), logn, x.shape[0] // n,
                       hi(q), lo(q), hi(mu), lo(mu), form, threads)
     return y
+
+
+def oracle_ntt_inverse(y: np.ndarray, t: np.ndarray, logn: int, q: int = Q_NTT,
+                       mu: int = MU_NTT) -> np.ndarray:
+    """Inverse of the in-place network for forward table t (the oracle's
+    restatement of bntt_ntt_inverse_dev); y holds batch*N elements."""
+    lib = oracle()
+    n = 1 << logn
+    y = np.ascontiguousarray(y, dtype=np.uint64).reshape(-1, 2)
+    t = np.ascontiguousarray(t, dtype=np.uint64).reshape(-1, 2)
+    assert y.shape[0] % n == 0 and t.shape[0] == n
+    x = np.empty_like(y)
+    rc = lib.orc_ntt_inverse_batch(_ptr(x), _ptr(y), _ptr(t), logn, y.shape[0] // n,
+                                   hi(q), lo(q), hi(mu), lo(mu))
+    assert rc == 0, "table entry or N not invertible"
+    return x
 
 
 def oracle_ntt_jobs(xs, ts, logns, q: int = Q_NTT, mu: int = MU_NTT, threads: int = 1):

@@ -171,3 +171,20 @@ def test_simd_reference_builds_agree_on_random_inputs(impl, logn):
     t = C.uniform_pairs(6 + logn, n, C.Q_NTT)
     assert np.array_equal(C.ref_ntt(x, t, logn, impl=impl, threads=2),
                           C.ref_ntt(x, t, logn, impl="scalar"))
+
+
+@pytest.mark.parametrize("logn", range(4, 11))
+def test_oracle_inverse_inverts_reference_goldens(logn):
+    """The inverse restatement (no reference counterpart) maps the reference's
+    golden outputs data/ver_N.txt back to its inputs data/x_N.txt."""
+    n = 1 << logn
+    assert np.array_equal(C.oracle_ntt_inverse(GOLD[f"ver_{n}"], GOLD[f"twd_{n}"], logn),
+                          GOLD[f"x_{n}"])
+
+
+@pytest.mark.parametrize("logn", [1, 2, 5, 12, 14])
+def test_oracle_inverse_round_trip(logn):
+    n = 1 << logn
+    x = C.uniform_pairs(300 + logn, 3 * n, C.Q_NTT)
+    t = C.uniform_pairs(400 + logn, n, C.Q_NTT)
+    assert np.array_equal(C.oracle_ntt_inverse(C.oracle_ntt(x, t, logn, form=1), t, logn), x)

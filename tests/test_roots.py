@@ -163,3 +163,29 @@ def test_fast_multiply_bound_widened():
         assert bn.lib().bntt_modulus_is_fast(ctypes.byref(bn.modulus(q))) == fast
     q = (1 << 124) - 0x7bfffff
     assert bn.lib().bntt_modulus_is_fast(ctypes.byref(bn.modulus(q, ((1 << 251) // q) - 1))) == 0
+
+
+@pytest.mark.parametrize("logn", [1, 3, 6])
+def test_oracle_inverse_is_inverse_negacyclic_dft(logn):
+    """With root-power tables the inverse network is
+    x[j] = N^-1 sum_i Y[i] psi^-((2 brv(i) + 1) j)."""
+    n = 1 << logn
+    psi = C.negacyclic_psi(Q_NC, logn)
+    y = C.uniform_pairs(61 + logn, n, Q_NC)
+    got = C.from_pairs(C.oracle_ntt_inverse(y, C.negacyclic_table(Q_NC, logn, psi), logn,
+                                            Q_NC, MU_NC))
+    ys, ninv, pinv = C.from_pairs(y), pow(n, Q_NC - 2, Q_NC), pow(psi, Q_NC - 2, Q_NC)
+    want = [ninv * sum(yi * pow(pinv, (2 * C.brv(i, logn) + 1) * j, Q_NC)
+                       for i, yi in enumerate(ys)) % Q_NC for j in range(n)]
+    assert got == want
+
+
+@pytest.mark.parametrize("logn", [4, 8])
+def test_oracle_polynomial_product(logn):
+    n = 1 << logn
+    t = C.negacyclic_table(Q_NC, logn, C.negacyclic_psi(Q_NC, logn))
+    a, b = C.uniform_pairs(71, n, Q_NC), C.uniform_pairs(72, n, Q_NC)
+    prod_hat = C.oracle_blas("vvmul", C.oracle_ntt(a, t, logn, Q_NC, MU_NC),
+                             C.oracle_ntt(b, t, logn, Q_NC, MU_NC), Q_NC, MU_NC)
+    got = C.oracle_ntt_inverse(prod_hat, t, logn, Q_NC, MU_NC)
+    assert C.from_pairs(got) == C.negacyclic_mul(C.from_pairs(a), C.from_pairs(b), Q_NC)
