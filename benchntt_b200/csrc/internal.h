@@ -140,4 +140,8 @@ int plan_create_common(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bntt_
 // b != nullptr fuses y = y * b into the last pass (MulB in ntt_core.cuh).
 int ntt_forward_on(bntt_plan* plan, void* y, const void* x, size_t batch, cudaStream_t s,
                    const void* b = nullptr, uint64_t bmask = 0);
+// The same on the runtime-size tile engine (fast multiply, log2n >= 3);
+// ntt_forward_on uses it above 2^10 points.
+int engine_forward_on(bntt_plan* plan, void* y, const void* x, size_t batch, cudaStream_t s,
+                      const void* b, uint64_t bmask);
 }  // namespace bntt

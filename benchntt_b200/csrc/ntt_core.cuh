@@ -63,6 +63,15 @@ struct MulB {
   uint64_t bmask = 0;
 };
 
+// What the last store of an engine kernel applies (ntt_engine.cuh): an
+// optional scalar multiply (the inverse transform's N^-1), then an optional
+// pointwise product (MulB).
+struct Epilogue {
+  U128 scale{};
+  int has_scale = 0;
+  MulB mul;
+};
+
 template <int M, int LOGR, int TPC, int MAP, class Arith>
 struct NttTile {
   static constexpr int R = 1 << LOGR;

@@ -72,12 +72,12 @@ struct NttEngine {
   //
   // INV runs the inverse of the same r stages: the stages in reverse order,
   // each an inverse (Gentleman-Sande) butterfly with the table holding the
-  // inverse twiddles, and on the last store an optional multiply by *scale.
-  template <int r, int LDP, bool INV = false>
+  // inverse twiddles.  EPI applies *ep (when not null) on the last store.
+  template <int r, int LDP, bool INV = false, bool EPI = false>
   __device__ __forceinline__ static void pass(U128 (&v)[R], const SubRef& sr, int s0, int lo,
                                               int lane, int tpt, bool first, bool last,
                                               const Layout& lay, uint4* smem, const ModParams& mp,
-                                              int layout, const U128* scale = nullptr) {
+                                              int layout, const Epilogue* ep = nullptr) {
     constexpr int G = 1 << r, GPT = R / G;
     const int hi_mask = ~((1 << lo) - 1);
     // group i's local index base: (g & lomask) | ((g >> lo) << (lo + r))
@@ -139,10 +139,17 @@ struct NttEngine {
         for (int j = 0; j < G; ++j) {
           const int idx = base(i) + (j << lo);
           if (sr.valid) {
-            if constexpr (INV) {
-              if (scale) v[i * G + j] = Arith::mul(v[i * G + j], *scale, mp);
+            uint4* yp = sr.y + ((size_t)idx << sr.lshift);
+            if constexpr (EPI) {
+              if (ep) {
+                if (ep->has_scale) v[i * G + j] = Arith::mul(v[i * G + j], ep->scale, mp);
+                if (ep->mul.b) {
+                  const uint4 bv = __ldg(ep->mul.b + ((uint64_t)(yp - ep->mul.ybase) & ep->mul.bmask));
+                  v[i * G + j] = Arith::mul(v[i * G + j], from_mem(bv, layout), mp);
+                }
+              }
             }
-            sr.y[(size_t)idx << sr.lshift] = to_mem(v[i * G + j], layout);
+            *yp = to_mem(v[i * G + j], layout);
           }
         }
       } else {
@@ -162,12 +169,12 @@ struct NttEngine {
   // Every thread of the CTA calls it; threads of invalid sub-transforms
   // compute on zeros and store nothing.
   //
-  // INV = true runs the inverse network of the same passes (last pass first)
-  // and multiplies the stored results by *scale when scale is not null.
-  template <int LDP, bool INV = false>
+  // INV = true runs the inverse network of the same passes (last pass
+  // first); EPI = true applies *ep (when not null) to the stored results.
+  template <int LDP, bool INV = false, bool EPI = false>
   __device__ __forceinline__ static void run(int M, int map, int threads, const SubRef& sr,
                                              int sub, int lane, uint4* smem, const ModParams& mp,
-                                             int layout, const U128* scale = nullptr) {
+                                             int layout, const Epilogue* ep = nullptr) {
     const Passes ps(M);
     const int tpt = 1 << (M - LOGR);
     const bool contig = map == MAP_CONTIG;
@@ -183,17 +190,17 @@ struct NttEngine {
       const bool first = pp == 0, last = pp == ps.n - 1;
       if constexpr (LOGR >= 4) {
         if (r == 4)
-          pass<(LOGR >= 4 ? 4 : 1), LDP, INV>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp,
-                                              layout, scale);
+          pass<(LOGR >= 4 ? 4 : 1), LDP, INV, EPI>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp,
+                                              layout, ep);
       }
       // with LOGR = 3 the balanced passes of 2^3..2^10 points have 2 or 3
       // stages, so width 1 needs no code there
       if (r == 3)
-        pass<3, LDP, INV>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout, scale);
+        pass<3, LDP, INV, EPI>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout, ep);
       else if (r == 2)
-        pass<2, LDP, INV>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout, scale);
+        pass<2, LDP, INV, EPI>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout, ep);
       else if (LOGR != 3)
-        pass<1, LDP, INV>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout, scale);
+        pass<1, LDP, INV, EPI>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout, ep);
       if (!last) {
         if (warp_local) __syncwarp();
         else __syncthreads();

@@ -1,4 +1,5 @@
-// inverse.cu -- inverse of the plan's forward transform.
+// ntt_engine_plan.cu -- plan transforms on the runtime-size tile engine:
+// the inverse transform, and the forward transform above 2^10 points.
 //
 // The reference has no inverse transform.  The forward network
 // (src/ntt_scalar.c:582-627, in its in-place form: stage s pairs indices
@@ -17,7 +18,10 @@
 //
 // Kernels: the runtime-size tile engine (ntt_engine.cuh) in inverse mode,
 // one launch per HBM pass in reverse pass order (the pass over the low index
-// bits first), and a one-thread-per-transform kernel for N = 2 and 4.
+// bits first), and a one-thread-per-transform kernel for N = 2 and 4.  The
+// same engine kernel in forward mode runs the plans' forward transforms
+// above 2^10 points (engine_forward_on): passes of at most 8 stages keep the
+// strided passes coalesced.
 #include <algorithm>
 #include <vector>
 
@@ -28,24 +32,28 @@
 namespace bntt {
 namespace {
 
-constexpr int kInvThreads = 256;
+constexpr int kEngThreads = 256;
 // Largest HBM pass: a strided pass of 2^m points then covers
 // 256 >> (m - 3) >= 8 adjacent columns (128 contiguous bytes per row).
-constexpr int kInvMaxPass = 8;
+constexpr int kEngMaxPass = 8;
 
-using InvEngine = NttEngine<3, ArithFast>;
+using PlanEngine = NttEngine<3, ArithFast>;
 
-__global__ void __launch_bounds__(kInvThreads, 3)
-    k_ntt_inv(SubGeom g, ModParams mp, int layout, int m, int map, U128 scale, int do_scale) {
+// One HBM pass of a plan transform on the tile engine: tiles of 256 threads,
+// persistent over the pass's tiles.  INV selects the inverse network; `ep`
+// is applied by the last store when use_ep is set.
+template <bool INV>
+__global__ void __launch_bounds__(kEngThreads, 3)
+    k_ntt_engine(SubGeom g, ModParams mp, int layout, int m, int map, Epilogue ep, int use_ep) {
   extern __shared__ uint4 smem[];
   int sub, lane;
-  InvEngine::place(threadIdx.x, m, map, kInvThreads, &sub, &lane);
-  const int tpc = kInvThreads >> (m - 3);
+  PlanEngine::place(threadIdx.x, m, map, kEngThreads, &sub, &lane);
+  const int tpc = kEngThreads >> (m - 3);
   const uint64_t ntiles = (g.nsub + (uint64_t)tpc - 1) / (uint64_t)tpc;
   for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const SubRef sr = make_subref(g, tile * (uint64_t)tpc + (uint64_t)sub);
-    InvEngine::run<LD_CG, true>(m, map, kInvThreads, sr, sub, lane, smem, mp, layout,
-                                do_scale ? &scale : nullptr);
+    PlanEngine::run<LD_CG, INV, true>(m, map, kEngThreads, sr, sub, lane, smem, mp, layout,
+                                      use_ep ? &ep : nullptr);
     __syncthreads();  // shared memory is reused by the next tile
   }
 }
@@ -70,15 +78,56 @@ __global__ void __launch_bounds__(256)
   for (int i = 0; i < N; ++i) x[t * N + i] = to_mem(ArithFast::mul(v[i], scale, mp), layout);
 }
 
-int inv_blocks_per_sm(size_t smem) {
+template <bool INV>
+int engine_blocks_per_sm(size_t smem) {
   static int cached[2] = {0, 0};
   const int slot = smem > 0 ? 1 : 0;
   if (cached[slot]) return cached[slot];
   int b = 0;
-  BNTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void*)k_ntt_inv, kInvThreads,
-                                                        smem));
+  const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &b, (const void*)k_ntt_engine<INV>, kEngThreads, smem);
+  if (e != cudaSuccess) return -cuda_error(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
   cached[slot] = std::max(1, b);
   return cached[slot];
+}
+
+// The HBM passes of a 2^n transform (n >= 3) on the engine: forward in pass
+// order, inverse in reverse order.  The first pass run reads `in`, every
+// pass writes `out` (in place after the first), and the last pass run
+// applies `ep` when use_ep is set.
+template <bool INV>
+int engine_passes(bntt_plan* p, void* out, const void* in, size_t batch, const void* tw,
+                  const Epilogue& ep, int use_ep, cudaStream_t s) {
+  const int n = (int)p->log2n;
+  const std::vector<int> passes = n <= 10 ? std::vector<int>{n} : split_passes(n, kEngMaxPass);
+  const int np = (int)passes.size();
+  std::vector<int> starts(np, 0);
+  for (int i = 1; i < np; ++i) starts[i] = starts[i - 1] + passes[i - 1];
+  for (int k = 0; k < np; ++k) {
+    const int i = INV ? np - 1 - k : k;
+    const int m = passes[i];
+    SubGeom g;
+    g.x = static_cast<const uint4*>(k == 0 ? in : out);
+    g.y = static_cast<uint4*>(out);
+    g.tw = static_cast<const uint4*>(tw);
+    g.n = (uint32_t)n;
+    g.s0 = (uint32_t)starts[i];
+    g.m = (uint32_t)m;
+    g.l = (uint32_t)(n - starts[i] - m);
+    g.nsub = (uint64_t)batch << (n - m);
+    const int map = g.l > 0 ? MAP_INTERLEAVED : MAP_CONTIG;
+    const size_t smem = PlanEngine::smem_slots(m, map, kEngThreads) * 16;
+    const int bps = engine_blocks_per_sm<INV>(smem);
+    if (bps < 0) return -bps;
+    const int tpc = kEngThreads >> (m - 3);
+    const uint64_t ntiles = (g.nsub + (uint64_t)tpc - 1) / (uint64_t)tpc;
+    const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)bps * p->ctx->sms);
+    k_ntt_engine<INV><<<grid, kEngThreads, smem, s>>>(g, p->mp, p->layout, m, map, ep,
+                                                      (k == np - 1 && use_ep) ? 1 : 0);
+    BNTT_CK(cudaGetLastError());
+    p->ctx->launches++;
+  }
+  return BNTT_OK;
 }
 
 // Inverse table (T[k]^-1, limb order) and N^-1, built once per plan: the
@@ -131,44 +180,34 @@ int ensure_inverse(bntt_plan* p) {
 
 int inverse_on(bntt_plan* p, void* x, const void* y, size_t batch, cudaStream_t s) {
   const int n = (int)p->log2n;
-  uint4* xo = static_cast<uint4*>(x);
-  const uint4* yi = static_cast<const uint4*>(y);
-  const uint4* tw = static_cast<const uint4*>(p->tw_inv);
   if (n <= 2) {
     const unsigned grid = (unsigned)((batch + 255) / 256);
-    k_ntt_inv_tiny<<<grid, 256, 0, s>>>(xo, yi, tw, (uint64_t)batch, n, p->mp, p->layout, p->ninv);
+    k_ntt_inv_tiny<<<grid, 256, 0, s>>>(static_cast<uint4*>(x), static_cast<const uint4*>(y),
+                                        static_cast<const uint4*>(p->tw_inv), (uint64_t)batch, n,
+                                        p->mp, p->layout, p->ninv);
     BNTT_CK(cudaGetLastError());
     p->ctx->launches++;
     return BNTT_OK;
   }
-  const std::vector<int> passes = n <= 10 ? std::vector<int>{n} : split_passes(n, kInvMaxPass);
-  std::vector<int> starts(passes.size(), 0);
-  for (size_t i = 1; i < passes.size(); ++i) starts[i] = starts[i - 1] + passes[i - 1];
-  for (int i = (int)passes.size() - 1; i >= 0; --i) {
-    const int m = passes[i];
-    SubGeom g;
-    g.x = i == (int)passes.size() - 1 ? yi : xo;  // first executed pass reads the input
-    g.y = xo;
-    g.tw = tw;
-    g.n = (uint32_t)n;
-    g.s0 = (uint32_t)starts[i];
-    g.m = (uint32_t)m;
-    g.l = (uint32_t)(n - starts[i] - m);
-    g.nsub = (uint64_t)batch << (n - m);
-    const int map = g.l > 0 ? MAP_INTERLEAVED : MAP_CONTIG;
-    const size_t smem = InvEngine::smem_slots(m, map, kInvThreads) * 16;
-    const int bps = inv_blocks_per_sm(smem);
-    const int tpc = kInvThreads >> (m - 3);
-    const uint64_t ntiles = (g.nsub + (uint64_t)tpc - 1) / (uint64_t)tpc;
-    const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)bps * p->ctx->sms);
-    k_ntt_inv<<<grid, kInvThreads, smem, s>>>(g, p->mp, p->layout, m, map, p->ninv, i == 0 ? 1 : 0);
-    BNTT_CK(cudaGetLastError());
-    p->ctx->launches++;
-  }
-  return BNTT_OK;
+  Epilogue ep;
+  ep.scale = p->ninv;
+  ep.has_scale = 1;
+  return engine_passes<true>(p, x, y, batch, p->tw_inv, ep, 1, s);
 }
 
 }  // namespace
+
+// Forward transform of a plan on the engine (fast multiply, n >= 3), with
+// the optional fused pointwise product of MulB on the last pass.
+int engine_forward_on(bntt_plan* p, void* y, const void* x, size_t batch, cudaStream_t s,
+                      const void* b, uint64_t bmask) {
+  Epilogue ep;
+  ep.mul.b = static_cast<const uint4*>(b);
+  ep.mul.ybase = static_cast<const uint4*>(y);
+  ep.mul.bmask = bmask;
+  return engine_passes<false>(p, y, x, batch, p->tw, ep, b ? 1 : 0, s);
+}
+
 }  // namespace bntt
 
 using namespace bntt;
