@@ -59,7 +59,7 @@ def parse():
                     help="fraction of the uneven batch (profiling captures of a smaller case)")
     ap.add_argument("--headline-only", action="store_true",
                     help="only the persistent-kernel step (for profiler launch lists)")
-    ap.add_argument("--only", choices=["uniform", "blas"], default=None,
+    ap.add_argument("--only", choices=["uniform", "inverse", "blas"], default=None,
                     help="run one secondary benchmark alone (profiling captures)")
     ap.add_argument("--logn", type=int, default=10, help="size for --only uniform")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -249,8 +249,9 @@ def run_only(args, dist: Dist):
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(device=dev)
     ctx = bn.Context(dev, stream=stream.cuda_stream)
-    if args.only == "uniform":
-        res = uniform_bench(args, ctx, stream, ctx.imad_peak(), sizes=[args.logn])
+    if args.only in ("uniform", "inverse"):
+        res = uniform_bench(args, ctx, stream, ctx.imad_peak(), sizes=[args.logn],
+                            inverse=args.only == "inverse")
     else:
         res = blas_bench(args, ctx, stream, measured_peaks())
     return {"only": args.only, "result": res}, ctx
@@ -531,29 +532,32 @@ def blas_bench(args, ctx, stream, peaks) -> dict:
     return res
 
 
-def uniform_bench(args, ctx, stream, imad_peak, sizes=range(4, 11)) -> dict:
-    """65,536 transforms of one size, one launch (config: uniform batch)."""
+def uniform_bench(args, ctx, stream, imad_peak, sizes=(4, 5, 6, 7, 8, 9, 10, 16, 20),
+                  inverse=False) -> dict:
+    """65,536 transforms of one size, one launch (config: uniform batch);
+    above 2^10 points, 2^26 elements.  inverse=True times the inverse."""
     import torch
 
     import benchntt_b200 as bn
     L = bn.lib()
     mod = bn.modulus(Q_NTT, MU_NTT)
     res = {}
-    count = 65536
     for logn in sizes:
         n = 1 << logn
+        count = 65536 if logn <= 10 else (1 << 26) >> logn
         x = torch.empty((n * count, 2), dtype=torch.int64, device=ctx.device)
         y = torch.empty_like(x)
         bn.check(L.bntt_fill_uniform_dev(ctx.handle, x.data_ptr(), n * count, 7, 0,
                                          ctypes.byref(mod), 0))
         plan = bn.Plan(ctx, logn, Q_NTT, MU_NTT, bn.fill_uniform(2000 + logn, n, Q_NTT))
+        run = (lambda: plan.inverse(y, x, count)) if inverse else (lambda: plan.forward(y, x, count))
         for _ in range(max(1, min(3, args.warmup))):
-            plan.forward(y, x, count)
+            run()
         e0, e1 = cuda_events()
         reps = max(1, args.steps // 2) if args.only else max(5, args.steps // 2)
         e0.record(stream)
         for _ in range(reps):
-            plan.forward(y, x, count)
+            run()
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / reps
