@@ -303,7 +303,7 @@ int bntt_batch_status(bntt_batch* b) {
 size_t bntt_batch_last_launches(bntt_batch* b) { return b ? b->last_launches : 0; }
 
 // Host buffers: jobs are packed into one device region (in place), split into
-// groups of about 1/8 of the bytes each.  Group g's inputs go up on one copy
+// groups of about 1/16 of the bytes each.  Group g's inputs go up on one copy
 // stream, its graph runs on the context stream, its outputs come back on the
 // other copy stream, so transfers of neighbouring groups overlap each other
 // and the kernels.  Host copies of jobs adjacent in host memory are merged.

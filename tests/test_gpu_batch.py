@@ -218,3 +218,64 @@ def test_bounded_wait_reports_timeout_and_context_stays_usable(ctx):
     assert s.engine.status() == bn.OK
     assert np.array_equal(s.output(), s.expected())
     s.close()
+
+
+def test_several_plans_per_size_scattered_buffers(ctx):
+    """Two tables for the same size, jobs in random order at scattered
+    (non-contiguous) offsets, several jobs reading the same input into
+    different outputs: every output equals the oracle's transform with its
+    own plan's table."""
+    rng = np.random.default_rng(17)
+    spec = [(3, 0), (8, 0), (8, 1), (12, 0), (12, 1), (17, 0)]   # (log2 N, table variant)
+    tables = [C.uniform_pairs(5000 + 10 * n + v, 1 << n, C.Q_NTT) for n, v in spec]
+    plans = [bn.Plan(ctx, n, C.Q_NTT, C.MU_NTT, t) for (n, _), t in zip(spec, tables)]
+    eng = bn.Batch(ctx, plans)
+    pick = rng.integers(0, len(spec), size=400)
+    pick[:3] = [5, 3, 4]                      # make sure the large plans are used
+    sizes = [1 << spec[p][0] for p in pick]
+    # inputs: one slot per job, some jobs re-use an earlier job's input
+    total_in = sum(sizes) + 4096
+    x = C.uniform_pairs(61, total_in, C.Q_NTT)
+    dx = DevBuf.from_array(ctx, x)
+    in_off, pos = [], 0
+    for i, n in enumerate(sizes):
+        if i > 10 and rng.random() < 0.1 and sizes[i - 1] == n:
+            in_off.append(in_off[-1])         # same input as the previous job
+        else:
+            pos += int(rng.integers(0, 3))    # gaps between inputs
+            in_off.append(pos)
+            pos += n
+    assert pos <= total_in
+    out_total = sum(sizes) * 2
+    dy = DevBuf(ctx, out_total * 16)
+    out_off, pos = [], 0
+    for n in sizes:
+        pos += int(rng.integers(0, 5))
+        out_off.append(pos)
+        pos += n
+    assert pos <= out_total
+    order = rng.permutation(len(sizes))
+    jobs = bn.Batch.jobs([dx.addr + 16 * in_off[i] for i in order],
+                         [dy.addr + 16 * out_off[i] for i in order], [int(pick[i]) for i in order])
+    eng.run_dev(jobs)
+    assert eng.status() == bn.OK
+    y = dy.to_array()
+    for i in range(len(sizes)):
+        p, n = int(pick[i]), sizes[i]
+        want = C.oracle_ntt(x[in_off[i]:in_off[i] + n], tables[p], spec[p][0], threads=8, form=1)
+        assert np.array_equal(y[out_off[i]:out_off[i] + n], want), f"job {i} (plan {p})"
+    dx.free()
+    dy.free()
+    eng.close()
+    for p in plans:
+        p.close()
+
+
+def test_empty_job_list(ctx):
+    p = bn.Plan(ctx, 5, C.Q_NTT, C.MU_NTT, C.uniform_pairs(1, 32, C.Q_NTT))
+    eng = bn.Batch(ctx, [p])
+    before = ctx.launches
+    eng.run_dev(bn.Batch.jobs([], [], []))
+    assert eng.status() == bn.OK and ctx.launches == before
+    eng.close()
+    p.close()
