@@ -47,24 +47,24 @@ struct NttEngine {
     }
   }
 
-  // Shared-memory slots (16 bytes each) of a tile.  Contiguous tiles give
-  // each sub-transform 2^M + 2^M/8 slots and pad one slot per 8:
-  //   slot = sub * (2^M + 2^M/8) + idx + (idx >> 3)
-  // which spreads the strided accesses of every pass over the banks, and
-  // because idx = base | (j << lo) has disjoint bits, slot(idx) =
-  // slot(base) + pad(j << lo): one add per element once the group's base is
-  // known.  Interleaved tiles use slot = idx * TPC + sub.
+  // Shared-memory slots (16 bytes each) of a tile.  Element idx of
+  // sub-transform `sub` has the linear index
+  //   contiguous tiles:  L = (sub << M) + idx
+  //   interleaved tiles: L = idx * TPC + sub
+  // and lives in slot L + (L >> 3): one pad slot per 8 spreads the strided
+  // accesses of every pass over the banks.  Within a pass, element j of a
+  // group is L(base) + j * (lmul << lo), so each element costs one
+  // multiply-add and one shifted add.
   __host__ __device__ static constexpr size_t smem_slots(int M, int map, int threads) {
-    return map == MAP_INTERLEAVED ? (size_t)threads * R
-                                  : (size_t)(threads >> (M - LOGR)) * (((size_t)1 << M) + ((size_t)1 << M >> 3));
+    (void)M;
+    (void)map;
+    return (size_t)threads * R + ((size_t)threads * R >> 3);
   }
 
   struct Layout {
-    int contig, tpc, sbase;
-    __device__ __forceinline__ int slot(int idx) const {
-      return contig ? sbase + idx + (idx >> 3) : idx * tpc + sbase;
-    }
+    int lbase, lmul;  // linear index L(idx) = lbase + idx * lmul
   };
+  __device__ __forceinline__ static int pad(int l) { return l + (l >> 3); }
 
   // One pass of width r (1 <= r <= LOGR) over the thread's GPT = R / 2^r
   // groups: gather (global on the first pass, else shared), r butterfly
@@ -80,6 +80,7 @@ struct NttEngine {
                                               int layout, const Epilogue* ep = nullptr) {
     constexpr int G = 1 << r, GPT = R / G;
     const int hi_mask = ~((1 << lo) - 1);
+    const int step = lay.lmul << lo;  // linear-index distance of j and j + 1
     // group i's local index base: (g & lomask) | ((g >> lo) << (lo + r))
     auto base = [&](int i) {
       const int g = lane + i * tpt;
@@ -100,11 +101,10 @@ struct NttEngine {
           }
         }
       } else {
-        const int sb = lay.slot(base(i));
+        const int lb = lay.lbase + base(i) * lay.lmul;
 #pragma unroll
         for (int j = 0; j < G; ++j) {
-          const int jo = j << lo;
-          const uint4 t = smem[sb + (lay.contig ? jo + (jo >> 3) : jo * lay.tpc)];
+          const uint4 t = smem[pad(lb + j * step)];
           v[i * G + j] = U128{{t.x, t.y, t.z, t.w}};
         }
       }
@@ -153,12 +153,11 @@ struct NttEngine {
           }
         }
       } else {
-        const int sb = lay.slot(base(i));
+        const int lb = lay.lbase + base(i) * lay.lmul;
 #pragma unroll
         for (int j = 0; j < G; ++j) {
-          const int jo = j << lo;
           const U128& e = v[i * G + j];
-          smem[sb + (lay.contig ? jo + (jo >> 3) : jo * lay.tpc)] =
+          smem[pad(lb + j * step)] =
               make_uint4(e.w[0], e.w[1], e.w[2], e.w[3]);
         }
       }
@@ -180,9 +179,8 @@ struct NttEngine {
     const bool contig = map == MAP_CONTIG;
     const bool warp_local = contig && tpt <= 32;
     Layout lay;
-    lay.contig = contig;
-    lay.tpc = threads >> (M - LOGR);
-    lay.sbase = contig ? sub * ((1 << M) + (1 << M >> 3)) : sub;
+    lay.lbase = contig ? sub << M : sub;
+    lay.lmul = contig ? 1 : threads >> (M - LOGR);
     U128 v[R];
     for (int pp = 0; pp < ps.n; ++pp) {
       const int p = INV ? ps.n - 1 - pp : pp;
