@@ -81,6 +81,7 @@ struct NttEngine {
     constexpr int G = 1 << r, GPT = R / G;
     const int hi_mask = ~((1 << lo) - 1);
     const int step = lay.lmul << lo;  // linear-index distance of j and j + 1
+    const uint32_t gstep = 1u << (lo + sr.lshift);  // the same in global memory
     // group i's local index base: (g & lomask) | ((g >> lo) << (lo + r))
     auto base = [&](int i) {
       const int g = lane + i * tpt;
@@ -90,11 +91,11 @@ struct NttEngine {
 #pragma unroll
     for (int i = 0; i < GPT; ++i) {
       if (first) {
+        const uint4* gp = sr.x + ((size_t)base(i) << sr.lshift);
 #pragma unroll
         for (int j = 0; j < G; ++j) {
-          const int idx = base(i) + (j << lo);
           if (sr.valid) {
-            v[i * G + j] = from_mem(ld_data<LDP>(sr.x + ((size_t)idx << sr.lshift)), layout);
+            v[i * G + j] = from_mem(ld_data<LDP>(gp + (size_t)(j * gstep)), layout);
           } else {
 #pragma unroll
             for (int w = 0; w < 4; ++w) v[i * G + j].w[w] = 0u;
@@ -135,11 +136,11 @@ struct NttEngine {
 #pragma unroll
     for (int i = 0; i < GPT; ++i) {
       if (last) {
+        uint4* const gq = sr.y + ((size_t)base(i) << sr.lshift);
 #pragma unroll
         for (int j = 0; j < G; ++j) {
-          const int idx = base(i) + (j << lo);
           if (sr.valid) {
-            uint4* yp = sr.y + ((size_t)idx << sr.lshift);
+            uint4* yp = gq + (size_t)(j * gstep);
             if constexpr (EPI) {
               if (ep) {
                 if (ep->has_scale) v[i * G + j] = Arith::mul(v[i * G + j], ep->scale, mp);
