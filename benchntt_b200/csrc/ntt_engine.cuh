@@ -26,7 +26,8 @@ struct NttEngine {
     int n, base, extra;
     __device__ __forceinline__ explicit Passes(int M) {
       n = (M + LOGR - 1) / LOGR;
-      base = M / n;
+      // M / n for n <= 4 and M <= 31 without a division instruction
+      base = n == 1 ? M : n == 2 ? M >> 1 : n == 3 ? (M * 11) >> 5 : M >> 2;
       extra = M - base * n;
     }
     __device__ __forceinline__ int bits(int p) const { return base + (p < extra ? 1 : 0); }
