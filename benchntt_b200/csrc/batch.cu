@@ -2,6 +2,7 @@
 // and the bntt_batch_* entry points.  Device code: batch_dev.cuh,
 // instantiated in batch_kfast.cu / batch_kref.cu.
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 
@@ -14,12 +15,12 @@ const void* batch_kernel_ref();
 
 // Resident CTAs per SM the fast batch kernel is compiled for (2 or 3); the
 // autotuner may change it.  BNTT_BATCH_MINB overrides it at start-up.
-static int g_batch_minb = [] {
+static std::atomic<int> g_batch_minb{[] {
   const char* e = getenv("BNTT_BATCH_MINB");
   return (e && atoi(e) == 2) ? 2 : 3;
-}();
-int batch_minb() { return g_batch_minb; }
-void set_batch_minb(int m) { g_batch_minb = m == 2 ? 2 : 3; }
+}()};
+int batch_minb() { return g_batch_minb.load(std::memory_order_relaxed); }
+void set_batch_minb(int m) { g_batch_minb.store(m == 2 ? 2 : 3, std::memory_order_relaxed); }
 
 size_t shape_smem(int s) {
   const BatchShape& b = kShapes[s];

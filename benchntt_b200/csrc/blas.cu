@@ -7,6 +7,7 @@
 // write).  No shared memory; the grid is up to 8 waves of resident blocks
 // and walks the vector with a grid-stride loop.
 #include <algorithm>
+#include <atomic>
 
 #include "internal.h"
 
@@ -64,19 +65,21 @@ int launch_blas(bntt_ctx* ctx, int op, void* c, const void* a, const void* b, U1
     case OP_AXPY: fn = fast ? blas_fn<OP_AXPY, ArithFast>() : blas_fn<OP_AXPY, ArithRef>(); break;
     default: return set_error(BNTT_EINVAL, "unknown BLAS op %d", op);
   }
-  static int bps_cache[8] = {0};
+  // resident blocks per SM of each kernel (the same on every B200); relaxed
+  // atomics because several host threads may launch at once
+  static std::atomic<int> bps_cache[8];
   const int slot = op * 2 + (fast ? 1 : 0);
-  if (bps_cache[slot] == 0) {
+  if (bps_cache[slot].load(std::memory_order_relaxed) == 0) {
     int b = 0;
     BNTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kBlasThreads, 0));
-    bps_cache[slot] = std::max(1, b);
+    bps_cache[slot].store(std::max(1, b), std::memory_order_relaxed);
   }
   const size_t per_block = (size_t)kBlasThreads * kBlasUnroll;
   const size_t blocks_needed = (len + per_block - 1) / per_block;
   // up to 8 waves of resident blocks: at 2^24 elements (805 MB per op) a
   // sweep of unroll x waves on B200 put 8 waves at 103-104 % of the measured
   // copy bandwidth for vvadd, vvmul and axpy, against 91-99 % at 2 waves
-  const size_t cap = (size_t)bps_cache[slot] * (size_t)ctx->sms * 8;
+  const size_t cap = (size_t)bps_cache[slot].load(std::memory_order_relaxed) * (size_t)ctx->sms * 8;
   const unsigned grid = (unsigned)std::min(blocks_needed, cap);
   uint4* cc = static_cast<uint4*>(c);
   const uint4* aa = static_cast<const uint4*>(a);

@@ -23,6 +23,7 @@
 // above 2^10 points (engine_forward_on): passes of at most 8 stages keep the
 // strided passes coalesced.
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include "internal.h"
@@ -80,15 +81,15 @@ __global__ void __launch_bounds__(256)
 
 template <bool INV>
 int engine_blocks_per_sm(size_t smem) {
-  static int cached[2] = {0, 0};
+  static std::atomic<int> cached[2];  // per smem class; relaxed: same value from any thread
   const int slot = smem > 0 ? 1 : 0;
-  if (cached[slot]) return cached[slot];
+  if (const int c = cached[slot].load(std::memory_order_relaxed)) return c;
   int b = 0;
   const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &b, (const void*)k_ntt_engine<INV>, kEngThreads, smem);
   if (e != cudaSuccess) return -cuda_error(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-  cached[slot] = std::max(1, b);
-  return cached[slot];
+  cached[slot].store(std::max(1, b), std::memory_order_relaxed);
+  return std::max(1, b);
 }
 
 // The HBM passes of a 2^n transform (n >= 3) on the engine: forward in pass
