@@ -825,6 +825,14 @@ def main():
             res["cpu_baseline"] = cpu_uneven_throughput(W.uneven_batch(), 12.0, cpu_threads())
             res["gpu_over_cpu"] = res["value"] / res["cpu_baseline"]["value"]
             res["e2e_over_cpu"] = res["e2e"]["value"] / res["cpu_baseline"]["value"]
+            # the same CPU sample per size: the reference's throughput on the
+            # uniform batches (all cores, one transform per core at a time)
+            cores = res["cpu_baseline"]["cores"]
+            for n, secs in res["cpu_baseline"].get("seconds_per_transform", {}).items():
+                row = res.get("uniform", {}).get(n)
+                if row and secs > 0:
+                    row["cpu_reference_ntt_per_s"] = cores / secs
+                    row["gpu_over_cpu"] = row["ntt_per_s"] / (cores / secs)
         if dist.rank == 0:
             print(json.dumps(res), flush=True)
         ctx.close()
