@@ -13,6 +13,7 @@ void append_fast_contig_r4(std::vector<SubKernel>& v);
 void append_fast_il(std::vector<SubKernel>& v);
 void append_ref(std::vector<SubKernel>& v);
 void append_fast_occ(std::vector<SubKernel>& v);
+void append_fast_small(std::vector<SubKernel>& v);
 
 const std::vector<SubKernel>& sub_kernels() {
   static std::vector<SubKernel> v = [] {
@@ -22,6 +23,7 @@ const std::vector<SubKernel>& sub_kernels() {
     append_fast_il(r);
     append_ref(r);
     append_fast_occ(r);
+    append_fast_small(r);
     return r;
   }();
   return v;
