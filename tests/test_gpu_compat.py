@@ -54,3 +54,13 @@ def test_blas_driver(tmp_path, datadir):
     assert out.returncode == 0, out.stdout + out.stderr
     assert out.stdout.split() == ["vvadd", "fail:", "0", "vvsub", "fail:", "0", "vvmul", "fail:",
                                   "0", "axpy", "fail:", "0"]
+
+
+@pytest.mark.parametrize("logn,batch", [(3, 3), (6, 2), (9, 1)])
+def test_polymul_driver(tmp_path, logn, batch):
+    """A C program on the native ABI: negacyclic products through forward,
+    fused pointwise product and inverse, against its own schoolbook product."""
+    exe = build(tmp_path, "polymul_driver.c")
+    out = subprocess.run([exe, str(logn), str(batch)], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.strip() == f"{1 << logn} fail: 0"
