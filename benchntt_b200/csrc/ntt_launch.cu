@@ -99,13 +99,15 @@ int plan_choose_kernels(bntt_plan* p) {
     // the tuned shape if the autotuner ran, else the first registered shape
     // that fits (interleaved tiles need TPC adjacent columns, so TPC <= 2^l)
     const SubKernel* k = tuned_sub_kernel(m, map, fast ? 1 : 0, l);
-    // untuned contiguous passes with the fast multiply: the shape capped at
-    // 3 resident CTAs per SM where one is compiled (the autotuner's pick for
-    // every such size on B200); without the cap the compiler spends up to
-    // 214 registers and one CTA fills the SM
-    for (const SubKernel& c : sub_kernels()) {
-      if (k || map != MAP_CONTIG || !fast) break;
-      if (c.m == m && c.map == map && c.fast == 1 && c.minb == 3) k = &c;
+    // untuned contiguous passes with the fast multiply: the 4-element shape
+    // capped at 4 resident CTAs per SM (2^3..2^8), else the shape capped at 3
+    // (2^9, 2^10) -- the autotuner's picks on B200; without a cap the
+    // compiler spends up to 214 registers and one CTA fills the SM
+    for (int want_minb : {4, 3}) {
+      for (const SubKernel& c : sub_kernels()) {
+        if (k || map != MAP_CONTIG || !fast) break;
+        if (c.m == m && c.map == map && c.fast == 1 && c.minb == want_minb) k = &c;
+      }
     }
     for (const SubKernel& c : sub_kernels()) {
       if (k) break;
