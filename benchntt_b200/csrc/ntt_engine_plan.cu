@@ -140,7 +140,10 @@ int ensure_inverse(bntt_plan* p) {
   const u128 q = to_u128(p->mod.q), mu = to_u128(p->mod.mu);
   const size_t n = (size_t)1 << p->log2n;
   std::vector<uint32_t> t(4 * n);
-  BNTT_CK(cudaMemcpy(t.data(), p->tw, n * 16, cudaMemcpyDeviceToHost));
+  // copies on the context's stream (ordered after any work that wrote the
+  // table, and finished before the first inverse launch reads the result)
+  BNTT_CK(cudaMemcpyAsync(t.data(), p->tw, n * 16, cudaMemcpyDeviceToHost, p->ctx->stream));
+  BNTT_CK(cudaStreamSynchronize(p->ctx->stream));
   auto entry = [&](size_t k) {
     u128 v = 0;
     for (int l = 3; l >= 0; --l) v = (v << 32) | t[4 * k + l];
@@ -169,10 +172,11 @@ int ensure_inverse(bntt_plan* p) {
   BNTT_REQUIRE(host_mulmod(ninv, (u128)n % q, q, mu) == 1, "N has no inverse mod q");
   void* d = nullptr;
   if (int rc = ctx_alloc(p->ctx, &d, n * 16)) return rc;
-  cudaError_t e = cudaMemcpy(d, ti.data(), n * 16, cudaMemcpyHostToDevice);
+  cudaError_t e = cudaMemcpyAsync(d, ti.data(), n * 16, cudaMemcpyHostToDevice, p->ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(p->ctx->stream);
   if (e != cudaSuccess) {
     ctx_free(p->ctx, d);
-    return cuda_error(e, "cudaMemcpy(inverse twiddles)");
+    return cuda_error(e, "copy of the inverse twiddles");
   }
   p->tw_inv = d;
   p->ninv = to_limbs(ninv);

@@ -395,10 +395,14 @@ int bntt_plan_create(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bntt_mo
       t[2 * i] = src[2 * i + 1];
       t[2 * i + 1] = src[2 * i];
     }
-    e = cudaMemcpy(p->tw, t.data(), bytes, cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(p->tw, t.data(), bytes, cudaMemcpyHostToDevice, c->stream);
   } else {
-    e = cudaMemcpy(p->tw, twiddles, bytes, cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(p->tw, twiddles, bytes, cudaMemcpyHostToDevice, c->stream);
   }
+  // on the context's (non-blocking) stream and complete before the plan is
+  // used: a plain cudaMemcpy from pageable memory may return before its DMA
+  // lands, and the default stream does not order it with that stream
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e == cudaSuccess) rc = plan_choose_kernels(p);
   else rc = cuda_error(e, "cudaMemcpy(twiddles)");
   if (rc) {
@@ -430,8 +434,11 @@ int bntt_plan_create_dev(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bnt
     p->own_tw = true;
     char* d = static_cast<char*>(p->tw);
     const char* s = static_cast<const char*>(twiddles_dev);
-    cudaError_t e = cudaMemcpy2D(d, 16, s + 8, 16, 8, n, cudaMemcpyDeviceToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy2D(d + 8, 16, s, 16, 8, n, cudaMemcpyDeviceToDevice);
+    // on the context's stream, finished before the plan is used
+    cudaError_t e = cudaMemcpy2DAsync(d, 16, s + 8, 16, 8, n, cudaMemcpyDeviceToDevice, c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(d + 8, 16, s, 16, 8, n, cudaMemcpyDeviceToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
       rc = cuda_error(e, "cudaMemcpy2D(twiddles)");
       ctx_free(c, p->tw);

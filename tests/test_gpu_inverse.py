@@ -141,3 +141,30 @@ def test_inverse_argument_errors(ctx):
     assert L.bntt_ntt_inverse_dev(p.handle, d.ptr, d.ptr, 0) == bn.OK
     d.free()
     p.close()
+
+
+@pytest.mark.parametrize("logn", [21, 22, 24])
+def test_round_trip_largest_sizes(ctx, logn):
+    """Up to the largest plan (2^24 points, three HBM passes of 8 stages each
+    way): ntt^-1(ntt(x)) = x for a random table, and the forward output is a
+    different vector."""
+    n = 1 << logn
+    t = C.uniform_pairs(2000 + logn, n, C.Q_NTT)
+    x = C.uniform_pairs(9100 + logn, n, C.Q_NTT)
+    p = bn.Plan(ctx, logn, C.Q_NTT, C.MU_NTT, t)
+    y = forward(ctx, p, x)
+    assert not np.array_equal(y, x)
+    assert np.array_equal(inverse(ctx, p, y), x)
+    p.close()
+
+
+def test_negacyclic_smallest_plan(ctx):
+    """N = 2: psi of order 4, one butterfly, against the oracle and back."""
+    psi = pow(ROOT21, 1 << (C.NC_LOG2_ORDER - 2), Q_NC)
+    p = bn.Plan.negacyclic(ctx, 1, Q_NC, MU_NC, psi)
+    x = C.uniform_pairs(5, 2 * 64, Q_NC)
+    t = C.negacyclic_table(Q_NC, 1, psi)
+    y = forward(ctx, p, x)
+    assert np.array_equal(y, C.oracle_ntt(x, t, 1, Q_NC, MU_NC))
+    assert np.array_equal(inverse(ctx, p, y), x)
+    p.close()
