@@ -404,7 +404,7 @@ int bntt_plan_create(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bntt_mo
   // lands, and the default stream does not order it with that stream
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e == cudaSuccess) rc = plan_choose_kernels(p);
-  else rc = cuda_error(e, "cudaMemcpy(twiddles)");
+  else rc = cuda_error(e, "copy of the twiddle table");
   if (rc) {
     ctx_free(c, p->tw);
     delete p;
@@ -440,7 +440,7 @@ int bntt_plan_create_dev(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bnt
       e = cudaMemcpy2DAsync(d + 8, 16, s, 16, 8, n, cudaMemcpyDeviceToDevice, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
-      rc = cuda_error(e, "cudaMemcpy2D(twiddles)");
+      rc = cuda_error(e, "copy of the twiddle table");
       ctx_free(c, p->tw);
       delete p;
       *out = nullptr;

@@ -95,3 +95,23 @@ def test_ctx_create_fails_cleanly_without_gpu():
     rc = bn.lib().bntt_ctx_create(ctypes.byref(h), 0, None)
     assert rc == bn.ENODEV and not h.value
     assert b"no CUDA device" in bn.lib().bntt_last_error()
+
+
+def test_no_unordered_copies_in_library_sources():
+    """Kernels run on each context's non-blocking stream.  A plain cudaMemcpy /
+    cudaMemcpy2D / cudaMemset goes to the legacy default stream, which is not
+    ordered with such a stream (and from pageable memory may return before the
+    data lands), so library code uses the Async forms on the context's stream.
+    The one plain copy allowed reads a status word after its stream was
+    synchronized."""
+    import glob
+    import re
+    allowed = {("batch.cu", "cudaMemcpy(&err")}
+    pat = re.compile(r"\b(cudaMemcpy|cudaMemcpy2D|cudaMemset)\(")
+    found = []
+    for path in sorted(glob.glob(os.path.join(C.ROOT, "benchntt_b200", "csrc", "*.cu"))):
+        for line in open(path):
+            if pat.search(line) and not any(os.path.basename(path) == f and tok in line
+                                            for f, tok in allowed):
+                found.append(f"{os.path.basename(path)}: {line.strip()}")
+    assert not found, found
