@@ -376,6 +376,8 @@ def run_ours(args, dist: Dist):
     result["blas"] = blas_bench(args, ctx, stream, peaks)
     # --------------------------------------------------------- uniform sizes
     result["uniform"] = uniform_bench(args, ctx, stream, imad_peak)
+    # ------------------------------------- inverse of the same batch, one launch
+    result["inverse_batch"] = inverse_batch_bench(args, ctx, stream, engine, jobs, batch, value)
     # --------------------------------- fused transform + pointwise product
     result["fused_mul"] = fused_bench(args, ctx, stream)
     # ------------------------------------------- NTT-friendly prime (negacyclic)
@@ -567,6 +569,25 @@ def uniform_bench(args, ctx, stream, imad_peak, sizes=(4, 5, 6, 7, 8, 9, 10, 16,
         plan.close()
         del x, y
     return res
+
+
+def inverse_batch_bench(args, ctx, stream, engine, jobs, batch, forward_value) -> dict:
+    """bntt_batch_run_inverse_dev on the headline job list: the inverse of
+    every transform of the uneven batch in one persistent launch."""
+    import torch
+    for _ in range(max(3, args.warmup)):
+        engine.run_inverse_dev(jobs)
+    e0, e1 = cuda_events()
+    reps = max(5, args.steps // 4)
+    e0.record(stream)
+    for _ in range(reps):
+        engine.run_inverse_dev(jobs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    return {"value": batch.count / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "vs_forward": batch.count / (ms * 1e-3) / forward_value,
+            "parity": "tests/test_gpu_batch.py::test_inverse_batch_matches_oracle"}
 
 
 def fused_bench(args, ctx, stream, sizes=(4, 7, 10, 16)) -> dict:

@@ -139,6 +139,7 @@ _SIGS = [
     ("bntt_batch_status", _I, [_P]),
     ("bntt_batch_inject_wait_timeout", _I, [_P, ctypes.c_uint32]),
     ("bntt_batch_last_launches", _S, [_P]),
+    ("bntt_batch_run_inverse_dev", _I, [_P, ctypes.POINTER(JobC), _S]),
     ("bntt_probe_imad_peak", _I, [_P, ctypes.POINTER(ctypes.c_double)]),
     ("bntt_probe_butterfly_peak", _I, [_P, ctypes.POINTER(ctypes.c_double)]),
     ("bntt_server_create", _I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _S, _PM,
@@ -418,6 +419,10 @@ class Batch:
 
     def run_host(self, jobs) -> None:
         check(lib().bntt_batch_run_host(self._h, jobs, len(jobs)))
+
+    def run_inverse_dev(self, jobs) -> None:
+        """Inverse transforms of the jobs (job.x -> job.y) in one launch."""
+        check(lib().bntt_batch_run_inverse_dev(self._h, jobs, len(jobs)))
 
     def run_percall_dev(self, jobs) -> None:
         """Each job as its own launch(es): the per-call comparison path."""

@@ -67,7 +67,8 @@ void free_schedule(bntt_ctx* c, Schedule& s) {
 
 const void* batch_kernel(bool fast) { return fast ? batch_kernel_fast_minb(g_batch_minb) : batch_kernel_ref(); }
 
-int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count) {
+int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count,
+                   bool inverse) {
   sc.djobs.resize(count);
   sc.order.clear();
   sc.items.clear();
@@ -84,7 +85,7 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
     DevJob& d = sc.djobs[i];
     d.x = static_cast<const uint4*>(jb.x);
     d.y = static_cast<uint4*>(jb.y);
-    d.tw = static_cast<const uint4*>(p->tw);
+    d.tw = static_cast<const uint4*>(inverse ? p->tw_inv : p->tw);
     d.log2n = p->log2n;
     d.slot = 0;
     if (p->log2n <= 10) {
@@ -111,6 +112,9 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
       const uint64_t nsub = 1ull << (n - m);
       const uint32_t tiles = (uint32_t)((nsub + tpc - 1) / tpc);
       sc.pass_tiles[d.slot * kMaxPasses + p] = tiles;
+      // position in the run order: forward pass p runs p-th, the inverse runs
+      // the passes last to first
+      const size_t run = inverse ? passes.size() - 1 - p : p;
       for (uint32_t t = 0; t < tiles; ++t) {
         WorkItem w{};
         w.shape = (uint16_t)shape;
@@ -118,13 +122,14 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
         w.a = ji;
         w.b = t * tpc;
         w.pass = (uint16_t)p;
-        w.wait = p > 0 ? 1 : 0;
-        later[p].push_back(w);
+        w.wait = run > 0 ? 1 : 0;
+        later[run].push_back(w);
       }
       s0 += m;
     }
   }
-  // queue: first passes, small tiles (largest size first), later passes
+  // queue: passes that run first, small tiles (largest size first), the
+  // other passes in run order
   for (const WorkItem& w : later[0]) sc.items.push_back(w);
   for (int n = 10; n >= 1; --n) {
     const std::vector<uint32_t>& v = by_size[n];
@@ -150,7 +155,8 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
 
 // Copies the schedule to the device and captures [memset control words,
 // kernel] into a graph on `stream`.
-static int upload_and_capture(bntt_batch* b, Schedule& sc, cudaStream_t stream) {
+static int upload_and_capture(bntt_batch* b, Schedule& sc, cudaStream_t stream,
+                              bool inverse = false) {
   bntt_ctx* c = b->ctx;
   const size_t jb = sc.djobs.size() * sizeof(DevJob), ob = sc.order.size() * 4,
                ib = sc.items.size() * sizeof(WorkItem), cb = (kCtlHeader + sc.nslots * kMaxPasses) * 4,
@@ -175,7 +181,7 @@ static int upload_and_capture(bntt_batch* b, Schedule& sc, cudaStream_t stream) 
     sc.exec = nullptr;
   }
   if (sc.items.empty()) return BNTT_OK;
-  const void* fn = batch_kernel(b->fast);
+  const void* fn = inverse ? batch_kernel_inverse() : batch_kernel(b->fast);
   size_t smem = 0;
   bool used[kNumShapes] = {};
   for (const WorkItem& w : sc.items) used[w.shape] = true;
@@ -197,7 +203,10 @@ static int upload_and_capture(bntt_batch* b, Schedule& sc, cudaStream_t stream) 
   ba.wait_polls = b->inject_polls ? b->inject_polls : kWaitPolls;
   ModParams mp = b->mp;
   int layout = b->layout;
-  void* args[] = {&ba, &mp, &layout};
+  InvScales scales{};
+  for (const bntt_plan* p : b->plans)
+    scales.ninv[p->log2n] = make_uint4(p->ninv.w[0], p->ninv.w[1], p->ninv.w[2], p->ninv.w[3]);
+  void* args[] = {&ba, &mp, &layout, &scales};  // the forward kernel takes the first three
   cudaGraph_t graph = nullptr;
   BNTT_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t e1 = cudaMemsetAsync(sc.d_ctl, 0, cb, stream);
@@ -267,6 +276,7 @@ int bntt_batch_destroy(bntt_batch* b) {
   cudaStreamSynchronize(c->stream);
   for (int s = 0; s < 2; ++s) cudaStreamSynchronize(c->copy_stream[s]);
   free_schedule(c, b->main);
+  free_schedule(c, b->inv);
   for (Schedule& s : b->groups) free_schedule(c, s);
   if (b->region) ctx_free(c, b->region);
   delete b;
@@ -291,11 +301,34 @@ int bntt_batch_run_dev(bntt_batch* b, const bntt_job* jobs, size_t count) {
   return launch_schedule(b, b->main, b->ctx->stream);
 }
 
+// Inverse transforms of a job list: same schedule machinery, the inverse
+// kernel, the plans' inverse tables (built on first use).
+int bntt_batch_run_inverse_dev(bntt_batch* b, const bntt_job* jobs, size_t count) {
+  BNTT_REQUIRE(b && (jobs || count == 0), "NULL argument");
+  if (int rc = ctx_use_device(b->ctx)) return rc;
+  b->last_launches = 0;
+  if (count == 0) return BNTT_OK;
+  BNTT_REQUIRE(b->fast, "the inverse transform needs q = 2^124 - k (k < 2^31), mu = floor(2^251/q) "
+               "and the default arithmetic");
+  for (bntt_plan* p : b->plans)
+    if (int rc = plan_ensure_inverse(p)) return rc;
+  const bool same = b->inv_last_jobs.size() == count && b->inv.exec_stream == b->ctx->stream &&
+                    memcmp(b->inv_last_jobs.data(), jobs, count * sizeof(bntt_job)) == 0;
+  if (!same) {
+    b->inv_last_jobs.clear();
+    if (int rc = build_schedule(b, b->inv, jobs, count, true)) return rc;
+    if (int rc = upload_and_capture(b, b->inv, b->ctx->stream, true)) return rc;
+    b->inv_last_jobs.assign(jobs, jobs + count);
+  }
+  return launch_schedule(b, b->inv, b->ctx->stream);
+}
+
 int bntt_batch_status(bntt_batch* b) {
   BNTT_REQUIRE(b, "NULL batch");
   if (int rc = ctx_use_device(b->ctx)) return rc;
   BNTT_CK(cudaStreamSynchronize(b->ctx->stream));
   if (int rc = schedule_status(b->main)) return rc;
+  if (int rc = schedule_status(b->inv)) return rc;
   for (Schedule& s : b->groups)
     if (int rc = schedule_status(s)) return rc;
   return BNTT_OK;

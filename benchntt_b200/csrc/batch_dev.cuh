@@ -112,6 +112,11 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
   return v;
 }
 
+// N^-1 mod q for each log2 N (limb order), for the inverse batch kernel.
+struct InvScales {
+  uint4 ninv[25];
+};
+
 struct BatchArgs {
   const WorkItem* items;
   uint32_t nitems;
@@ -125,7 +130,10 @@ struct BatchArgs {
 // The sub-transform a work item hands to thread `sub` of the tile: a whole
 // small job, or one sub-transform of an HBM pass of a large job.  Returns
 // false when the item is a later pass whose wait for its predecessor gave up
-// (the error word is set; the tile is skipped).
+// (the error word is set; the tile is skipped).  INV: the passes of a large
+// job run last to first (inverse transform), so a pass waits for the pass
+// after it and the last pass is the one that reads the job's input.
+template <bool INV = false>
 __device__ __forceinline__ bool item_subref(const WorkItem& it, const BatchArgs& ba, int m, int sub,
                                             int* s_flag, SubRef* out) {
   if (it.kind == ITEM_SMALL) {
@@ -147,11 +155,12 @@ __device__ __forceinline__ bool item_subref(const WorkItem& it, const BatchArgs&
   for (int p = 0; p < (int)it.pass; ++p) s0 += n / k + (p < n % k ? 1 : 0);
   if (it.wait) {
     uint32_t* counters = ba.ctl + kCtlHeader + j.slot * kMaxPasses;
+    const int pred = INV ? (int)it.pass + 1 : (int)it.pass - 1;
     if (threadIdx.x == 0) {
-      const uint32_t want = ba.pass_tiles[j.slot * kMaxPasses + it.pass - 1];
+      const uint32_t want = ba.pass_tiles[j.slot * kMaxPasses + pred];
       uint32_t polls = 0;
       int ok = 1;
-      while (ld_acquire(&counters[it.pass - 1]) < want) {
+      while (ld_acquire(&counters[pred]) < want) {
         if (++polls > ba.wait_polls) {
           atomicOr(&ba.ctl[1], 1u);
           ok = 0;
@@ -165,7 +174,8 @@ __device__ __forceinline__ bool item_subref(const WorkItem& it, const BatchArgs&
     if (!*s_flag) return false;
   }
   SubGeom g;
-  g.x = it.pass == 0 ? j.x : j.y;
+  if constexpr (INV) g.x = (int)it.pass == k - 1 ? j.x : j.y;
+  else g.x = it.pass == 0 ? j.x : j.y;
   g.y = j.y;
   g.tw = j.tw;
   g.n = (uint32_t)n;

@@ -57,6 +57,9 @@ struct bntt_batch {
   size_t last_launches = 0;
   // fault injection for tests of the failure path (bntt_batch_inject_wait_timeout)
   uint32_t inject_polls = 0;
+  // inverse runs (bntt_batch_run_inverse_dev)
+  std::vector<bntt_job> inv_last_jobs;
+  bntt::Schedule inv;
 };
 
 
@@ -64,6 +67,10 @@ namespace bntt {
 int grow(bntt_ctx* c, void** p, size_t* cap, size_t bytes);
 void free_schedule(bntt_ctx* c, Schedule& s);
 const void* batch_kernel(bool fast);
+const void* batch_kernel_inverse();
 size_t shape_smem(int s);
-int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count);
+// inverse = true: the jobs' inverse transforms (plans' inverse tables, the
+// passes of a large job queued last to first)
+int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count,
+                   bool inverse = false);
 }  // namespace bntt

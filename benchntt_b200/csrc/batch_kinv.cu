@@ -1,0 +1,88 @@
+// batch_kinv.cu -- the persistent batch kernel for inverse transforms
+// (bntt_batch_run_inverse_dev).  Same work queue and items as k_batch; each
+// item runs the inverse network (ntt_engine.cuh in inverse mode, stages last
+// to first with the plans' inverse tables), the passes of a large job run
+// from the last to the first, and whatever finishes a transform -- a small
+// tile, or pass 0 of a large job -- multiplies by N^-1 as it stores.
+// Fast moduli only, like the plans' inverse.
+#include "batch_dev.cuh"
+
+namespace bntt {
+
+namespace {
+
+// 2^1, 2^2: one thread per transform.
+template <int M>
+__device__ __noinline__ void run_item_tiny_inv(const WorkItem& it, const BatchArgs& ba,
+                                               const ModParams& mp, int layout,
+                                               const InvScales& sc, int* s_flag) {
+  SubRef sr;
+  if (!item_subref<true>(it, ba, M, threadIdx.x, s_flag, &sr)) return;
+  if (!sr.valid) return;
+  constexpr int N = 1 << M;
+  U128 v[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) v[i] = from_mem(__ldcg(sr.x + i), layout);
+#pragma unroll
+  for (int s = M - 1; s >= 0; --s) {
+    const int half = N >> (s + 1);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      if (i & half) continue;
+      const uint4 tv = __ldg(sr.tw + (1 << s) + (i >> (M - s)));
+      gs_butterfly<ArithFast>(v[i], v[i + half], U128{{tv.x, tv.y, tv.z, tv.w}}, mp);
+    }
+  }
+  const uint4 f = sc.ninv[M];
+  const U128 ninv = U128{{f.x, f.y, f.z, f.w}};
+#pragma unroll
+  for (int i = 0; i < N; ++i) sr.y[i] = to_mem(ArithFast::mul(v[i], ninv, mp), layout);
+}
+
+__device__ __noinline__ void run_item_engine_inv(const WorkItem& it, const BatchArgs& ba, uint4* smem,
+                                                 const ModParams& mp, int layout,
+                                                 const InvScales& sc, int* s_flag) {
+  using E = NttEngine<3, ArithFast>;
+  int m, map;
+  shape_of(it.shape, &m, &map);
+  int sub, lane;
+  E::place(threadIdx.x, m, map, kBatchThreads, &sub, &lane);
+  SubRef sr;
+  if (!item_subref<true>(it, ba, m, sub, s_flag, &sr)) return;
+  // the store that finishes a transform applies N^-1
+  const bool finishes = it.kind == ITEM_SMALL || it.pass == 0;
+  Epilogue ep;
+  if (finishes) {
+    const uint4 f = sc.ninv[it.kind == ITEM_SMALL ? m : (int)ba.jobs[it.a].log2n];
+    ep.scale = U128{{f.x, f.y, f.z, f.w}};
+    ep.has_scale = 1;
+  }
+  E::template run<LD_CG, true, true>(m, map, kBatchThreads, sr, sub, lane, smem, mp, layout,
+                                     finishes ? &ep : nullptr);
+  item_publish(it, ba);
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(kBatchThreads, MINB)
+    k_batch_inv(BatchArgs ba, ModParams mp, int layout, InvScales sc) {
+  extern __shared__ uint4 smem[];
+  __shared__ uint32_t s_item;
+  __shared__ int s_flag;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(&ba.ctl[0], 1u);
+    __syncthreads();
+    const uint32_t i = s_item;
+    if (i >= ba.nitems) break;
+    const WorkItem it = ba.items[i];
+    if (it.shape == 0) run_item_tiny_inv<1>(it, ba, mp, layout, sc, &s_flag);
+    else if (it.shape == 1) run_item_tiny_inv<2>(it, ba, mp, layout, sc, &s_flag);
+    else run_item_engine_inv(it, ba, smem, mp, layout, sc, &s_flag);
+    __syncthreads();  // smem and s_item are reused by the next item
+  }
+}
+
+}  // namespace
+
+const void* batch_kernel_inverse() { return (const void*)&k_batch_inv<3>; }
+
+}  // namespace bntt

@@ -135,6 +135,8 @@ int ctx_free(bntt_ctx* ctx, void* p);
 int ctx_use_device(bntt_ctx* ctx);
 bool arith_fast(bntt_ctx* ctx, bool modulus_fast);
 int plan_choose_kernels(bntt_plan* p);
+// Builds the plan's inverse table and N^-1 on first use (fast moduli only).
+int plan_ensure_inverse(bntt_plan* p);
 int plan_create_common(bntt_ctx* c, bntt_plan** out, unsigned log2n, const bntt_modulus* m,
                        int layout);
 // b != nullptr fuses y = y * b into the last pass (MulB in ntt_core.cuh).

@@ -202,6 +202,11 @@ int inverse_on(bntt_plan* p, void* x, const void* y, size_t batch, cudaStream_t 
 
 }  // namespace
 
+int plan_ensure_inverse(bntt_plan* p) {
+  if (!p->fast) return set_error(BNTT_EINVAL, "the inverse transform needs q = 2^124 - k (k < 2^31), mu = floor(2^251/q)");
+  return ensure_inverse(p);
+}
+
 // Forward transform of a plan on the engine (fast multiply, n >= 3), with
 // the optional fused pointwise product of MulB on the last pass.
 int engine_forward_on(bntt_plan* p, void* y, const void* x, size_t batch, cudaStream_t s,

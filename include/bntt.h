@@ -219,6 +219,14 @@ int bntt_batch_run_host(bntt_batch *batch, const bntt_job *jobs, size_t count);
  * most 1024 points, one per HBM pass above): the per-call path the
  * persistent kernel is compared with.  Device pointers, asynchronous. */
 int bntt_batch_run_percall_dev(bntt_batch *batch, const bntt_job *jobs, size_t count);
+/* Inverse transforms of a job list (the inverse of bntt_batch_run_dev for
+ * each job: x = ntt^-1(y) with job.x the input and job.y the output), in one
+ * persistent launch like the forward batch.  The inverse of the reference's
+ * network has no counterpart in the reference; see bntt_ntt_inverse_dev for
+ * its definition.  Needs the fast multiply and the default arithmetic; the
+ * plans' inverse tables are built on the first call. */
+int bntt_batch_run_inverse_dev(bntt_batch *batch, const bntt_job *jobs, size_t count);
+
 /* Same as bntt_batch_run_dev, but allocates no device memory: for callers
  * that cannot call cudaMalloc when they submit work (device memory owned by
  * another allocator's pool, latency-critical paths where an allocation would

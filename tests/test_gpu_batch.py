@@ -279,3 +279,54 @@ def test_empty_job_list(ctx):
     assert eng.status() == bn.OK and ctx.launches == before
     eng.close()
     p.close()
+
+
+def test_inverse_batch_matches_oracle(ctx):
+    """bntt_batch_run_inverse_dev: every job of a mix of 2^1..2^10 plus 2^12,
+    2^16 and 2^20 equals the oracle's inverse (orc_ntt_inverse_batch) of its
+    input, bit for bit."""
+    b = W.uneven_batch(seed=31, n_small=2500, small_lo=1, small_hi=10,
+                       large=((12, 2), (16, 2), (20, 1)))
+    s = Setup(ctx, b)
+    s.engine.run_inverse_dev(s.jobs())
+    assert s.engine.status() == bn.OK
+    got = s.output()
+    for i in range(b.count):
+        o, logn = int(b.offsets[i]), int(b.logns[i])
+        n = 1 << logn
+        want = C.oracle_ntt_inverse(s.x[o:o + n], s.tables[logn], logn)
+        assert np.array_equal(got[o:o + n], want), f"job {i} (2^{logn})"
+    s.close()
+
+
+def test_forward_then_inverse_batch_round_trip(ctx):
+    """Forward batch into y, inverse batch of y back: the inputs return, for
+    the uneven mix with large transforms (both directions one launch)."""
+    b = W.uneven_batch(seed=32, n_small=5000, large=((16, 4), (20, 2)))
+    s = Setup(ctx, b)
+    s.engine.run_dev(s.jobs())
+    zs = DevBuf(ctx, b.total * 16)
+    offs = [16 * int(o) for o in b.offsets]
+    back = bn.Batch.jobs([s.dy.addr + o for o in offs], [zs.addr + o for o in offs],
+                         [s.plan_ids[int(n)] for n in b.logns])
+    s.engine.run_inverse_dev(back)
+    assert s.engine.status() == bn.OK
+    assert np.array_equal(zs.to_array(), s.x)
+    assert s.engine.last_launches == 1
+    zs.free()
+    s.close()
+
+
+def test_inverse_batch_rejects_slow_modulus():
+    q = (1 << 123) + 12345678901
+    c = bn.Context(0)
+    p = bn.Plan(c, 5, q, (1 << 251) // q, C.uniform_pairs(1, 32, q))
+    eng = bn.Batch(c, [p])
+    d = DevBuf(c, 32 * 16)
+    with pytest.raises(bn.BnttError) as e:
+        eng.run_inverse_dev(bn.Batch.jobs([d.addr], [d.addr], [0]))
+    assert e.value.status == bn.EINVAL
+    d.free()
+    eng.close()
+    p.close()
+    c.close()
