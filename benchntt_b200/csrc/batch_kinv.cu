@@ -57,7 +57,7 @@ __device__ __noinline__ void run_item_engine_inv(const WorkItem& it, const Batch
     ep.scale = U128{{f.x, f.y, f.z, f.w}};
     ep.has_scale = 1;
   }
-  E::template run<LD_CG, true, true>(m, map, kBatchThreads, sr, sub, lane, smem, mp, layout,
+  E::template run<LD_CG, true, EPI_SCALE>(m, map, kBatchThreads, sr, sub, lane, smem, mp, layout,
                                      finishes ? &ep : nullptr);
   item_publish(it, ba);
 }

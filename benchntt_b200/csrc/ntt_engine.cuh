@@ -17,6 +17,8 @@
 
 namespace bntt {
 
+enum : int { EPI_SCALE = 1, EPI_MUL = 2 };
+
 template <int LOGR, class Arith>
 struct NttEngine {
   static constexpr int R = 1 << LOGR;
@@ -73,8 +75,9 @@ struct NttEngine {
   //
   // INV runs the inverse of the same r stages: the stages in reverse order,
   // each an inverse (Gentleman-Sande) butterfly with the table holding the
-  // inverse twiddles.  EPI applies *ep (when not null) on the last store.
-  template <int r, int LDP, bool INV = false, bool EPI = false>
+  // inverse twiddles.  EPI applies *ep (when not null) on the last store:
+  // bit EPI_SCALE its scalar multiply, bit EPI_MUL its pointwise product.
+  template <int r, int LDP, bool INV = false, int EPI = 0>
   __device__ __forceinline__ static void pass(U128 (&v)[R], const SubRef& sr, int s0, int lo,
                                               int lane, int tpt, bool first, bool last,
                                               const Layout& lay, uint4* smem, const ModParams& mp,
@@ -142,10 +145,12 @@ struct NttEngine {
         for (int j = 0; j < G; ++j) {
           if (sr.valid) {
             uint4* yp = gq + (size_t)(j * gstep);
-            if constexpr (EPI) {
+            if constexpr (EPI != 0) {
               if (ep) {
-                if (ep->has_scale) v[i * G + j] = Arith::mul(v[i * G + j], ep->scale, mp);
-                if (ep->mul.b) {
+                if constexpr ((EPI & EPI_SCALE) != 0) {
+                  if (ep->has_scale) v[i * G + j] = Arith::mul(v[i * G + j], ep->scale, mp);
+                }
+                if ((EPI & EPI_MUL) != 0 && ep->mul.b) {
                   const uint4 bv = __ldg(ep->mul.b + ((uint64_t)(yp - ep->mul.ybase) & ep->mul.bmask));
                   v[i * G + j] = Arith::mul(v[i * G + j], from_mem(bv, layout), mp);
                 }
@@ -171,8 +176,9 @@ struct NttEngine {
   // compute on zeros and store nothing.
   //
   // INV = true runs the inverse network of the same passes (last pass
-  // first); EPI = true applies *ep (when not null) to the stored results.
-  template <int LDP, bool INV = false, bool EPI = false>
+  // first); EPI (EPI_SCALE | EPI_MUL bits) applies *ep (when not null) to the
+  // stored results.
+  template <int LDP, bool INV = false, int EPI = 0>
   __device__ __forceinline__ static void run(int M, int map, int threads, const SubRef& sr,
                                              int sub, int lane, uint4* smem, const ModParams& mp,
                                              int layout, const Epilogue* ep = nullptr) {

@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(kEngThreads, 3)
   const uint64_t ntiles = (g.nsub + (uint64_t)tpc - 1) / (uint64_t)tpc;
   for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const SubRef sr = make_subref(g, tile * (uint64_t)tpc + (uint64_t)sub);
-    PlanEngine::run<LD_CG, INV, true>(m, map, kEngThreads, sr, sub, lane, smem, mp, layout,
+    PlanEngine::run<LD_CG, INV, INV ? EPI_SCALE : EPI_MUL>(m, map, kEngThreads, sr, sub, lane, smem, mp, layout,
                                       use_ep ? &ep : nullptr);
     __syncthreads();  // shared memory is reused by the next tile
   }
