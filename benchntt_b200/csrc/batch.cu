@@ -100,7 +100,7 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
   for (uint32_t ji : large) {
     const DevJob& d = sc.djobs[ji];
     const int n = (int)d.log2n;
-    const std::vector<int> passes = split_passes(n, kBatchMaxPass);
+    const std::vector<int> passes = engine_split(n);
     BNTT_REQUIRE(passes.size() <= (size_t)kMaxPasses, "log2n %d needs too many passes", n);
     int s0 = 0;
     for (size_t p = 0; p < passes.size(); ++p) {
@@ -122,7 +122,7 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
         w.a = ji;
         w.b = t * tpc;
         w.pass = (uint16_t)p;
-        w.wait = run > 0 ? 1 : 0;
+        w.wait = (uint16_t)((run > 0 ? 1 : 0) | (run == 0 ? 2 : 0) | (s0 << 8));
         later[run].push_back(w);
       }
       s0 += m;

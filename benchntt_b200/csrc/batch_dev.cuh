@@ -5,8 +5,9 @@
 //   SMALL   TPC transforms of one size 2^n <= 1024, taken from a list of
 //           jobs sorted by size (one sub-transform per job)
 //   PASS p  TPC sub-transforms of HBM pass p of one large transform
-//           (n > 10, passes of at most kBatchMaxPass stages: 2^16 = 8 + 8,
-//           2^20 = 7 + 7 + 6, so strided passes keep >= 8 adjacent columns)
+//           (n > 10, passes from engine_split: at most kBatchMaxPass stages
+//           so strided passes keep >= 8 adjacent columns, and the fewest
+//           engine passes: 2^16 = 8 + 8, 2^20 = 8 + 6 + 6)
 // A CTA takes the next item with an atomic counter.  Queue order is: all
 // first passes of large jobs, then small tiles from the largest size down,
 // then later passes.  Pass p > 0 of a job reads what pass p-1 wrote, so its
@@ -27,9 +28,9 @@
 namespace bntt {
 
 constexpr int kBatchThreads = 256;
-// Largest HBM pass of a large transform in the persistent kernel: a strided
-// pass of 2^m points has 256 >> (m - 3) adjacent columns per tile, and at
-// least 8 (128 contiguous bytes per row) keep its loads coalesced.
+// Largest HBM pass of a large transform (engine_split): a strided pass of
+// 2^m points has 256 >> (m - 3) adjacent columns per tile, and at least 8
+// (128 contiguous bytes per row) keep its loads coalesced.
 constexpr int kBatchMaxPass = 8;
 
 struct DevJob {
@@ -48,7 +49,8 @@ struct WorkItem {
   uint32_t a;       // SMALL: first position in the size-sorted order; PASS: job index
   uint32_t b;       // SMALL: number of jobs in the tile; PASS: first sub-transform id
   uint16_t pass;    // PASS: pass index
-  uint16_t wait;    // PASS: 1 if the tile waits for the previous pass
+  uint16_t wait;    // PASS: bit 0 the tile waits for the pass run before it,
+                    // bit 1 the pass reads the job's input, bits 8.. its first stage
 };
 static_assert(sizeof(WorkItem) == 16, "work item layout");
 
@@ -150,10 +152,8 @@ __device__ __forceinline__ bool item_subref(const WorkItem& it, const BatchArgs&
   }
   const DevJob& j = ba.jobs[it.a];
   const int n = (int)j.log2n;
-  const int k = (n + kBatchMaxPass - 1) / kBatchMaxPass;  // split_passes(n, kBatchMaxPass)
-  int s0 = 0;
-  for (int p = 0; p < (int)it.pass; ++p) s0 += n / k + (p < n % k ? 1 : 0);
-  if (it.wait) {
+  const int s0 = it.wait >> 8;  // first stage of this pass (engine_split on the host)
+  if (it.wait & 1) {
     uint32_t* counters = ba.ctl + kCtlHeader + j.slot * kMaxPasses;
     const int pred = INV ? (int)it.pass + 1 : (int)it.pass - 1;
     if (threadIdx.x == 0) {
@@ -174,8 +174,7 @@ __device__ __forceinline__ bool item_subref(const WorkItem& it, const BatchArgs&
     if (!*s_flag) return false;
   }
   SubGeom g;
-  if constexpr (INV) g.x = (int)it.pass == k - 1 ? j.x : j.y;
-  else g.x = it.pass == 0 ? j.x : j.y;
+  g.x = (it.wait & 2) ? j.x : j.y;
   g.y = j.y;
   g.tw = j.tw;
   g.n = (uint32_t)n;

@@ -82,6 +82,9 @@ int tuned_batch_small_shape(int m);
 // Pass decomposition of a 2^n transform: sizes of HBM passes (each <= max_m).
 // Plans use max_m = 10; the persistent kernel uses kBatchMaxPass.
 std::vector<int> split_passes(int n, int max_m = 10);
+// HBM passes of a 2^n transform (n > 10) on the tile engine (batch kernel,
+// engine plans): fewest passes of <= 8 stages, then fewest engine passes.
+std::vector<int> engine_split(int n);
 
 int launch_blas(bntt_ctx* ctx, int op, void* c, const void* a, const void* b, U128 x, size_t len,
                 const ModParams& mp, bool fast, int layout, cudaStream_t stream);

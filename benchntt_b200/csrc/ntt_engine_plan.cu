@@ -33,10 +33,10 @@
 namespace bntt {
 namespace {
 
+// Tiles of 256 threads; the HBM passes of a large transform come from
+// engine_split (at most 8 stages each, so a strided tile covers at least 8
+// adjacent columns: 128 contiguous bytes per row).
 constexpr int kEngThreads = 256;
-// Largest HBM pass: a strided pass of 2^m points then covers
-// 256 >> (m - 3) >= 8 adjacent columns (128 contiguous bytes per row).
-constexpr int kEngMaxPass = 8;
 
 using PlanEngine = NttEngine<3, ArithFast>;
 
@@ -100,7 +100,7 @@ template <bool INV>
 int engine_passes(bntt_plan* p, void* out, const void* in, size_t batch, const void* tw,
                   const Epilogue& ep, int use_ep, cudaStream_t s) {
   const int n = (int)p->log2n;
-  const std::vector<int> passes = n <= 10 ? std::vector<int>{n} : split_passes(n, kEngMaxPass);
+  const std::vector<int> passes = n <= 10 ? std::vector<int>{n} : engine_split(n);
   const int np = (int)passes.size();
   std::vector<int> starts(np, 0);
   for (int i = 1; i < np; ++i) starts[i] = starts[i - 1] + passes[i - 1];

@@ -1,6 +1,7 @@
 // ntt_launch.cu -- registry of compiled sub-transform kernels, the HBM pass
 // split, and the stream-ordered forward transform.
 #include <algorithm>
+#include <functional>
 #include <mutex>
 
 #include "internal.h"
@@ -84,6 +85,47 @@ std::vector<int> split_passes(int n, int max_m) {
   const int k = (n + max_m - 1) / max_m;
   for (int i = 0; i < k; ++i) p.push_back(n / k + (i < n % k ? 1 : 0));
   return p;
+}
+
+// Split of a 2^n transform (n > 10) for the tile engine: the fewest HBM
+// passes of at most 8 stages, and among those the split with the fewest
+// engine passes (each engine pass covers at most 3 stages, so a pass of 6
+// stages costs 2 and one of 7 costs 3), then the widest first pass.  For
+// 2^20 that is 8 + 6 + 6 (7 engine passes) instead of 7 + 7 + 6 (8).
+std::vector<int> engine_split(int n) {
+  const int k = (n + 7) / 8;
+  std::vector<int> best, cur(k, 0);
+  int best_cost = 1 << 30;
+  // enumerate compositions of n into k parts in [1, 8], first part largest first
+  std::vector<int> stack;
+  std::function<void(int, int)> rec = [&](int i, int left) {
+    if (i == k - 1) {
+      if (left < 1 || left > 8) return;
+      cur[i] = left;
+      int cost = 0, s0 = 0;
+      for (int j = 0; j < k; ++j) {
+        const int m = cur[j], l = n - s0 - m;
+        if (m < 3) return;  // the engine needs >= 2^3 points
+        // a strided pass: at least 2^5 points (the interleaved tile shapes),
+        // and its 256 >> (m - 3) columns per tile must exist (<= 2^l)
+        if (l > 0 && (m < 5 || 11 - m > l)) return;
+        cost += (m + 2) / 3;
+        s0 += m;
+      }
+      if (cost < best_cost) {
+        best_cost = cost;
+        best = cur;
+      }
+      return;
+    }
+    for (int m = 8; m >= 1; --m) {
+      if (left - m < (k - 1 - i) || left - m > 8 * (k - 1 - i)) continue;
+      cur[i] = m;
+      rec(i + 1, left - m);
+    }
+  };
+  rec(0, n);
+  return best;
 }
 
 int plan_choose_kernels(bntt_plan* p) {
