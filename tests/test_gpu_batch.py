@@ -330,3 +330,30 @@ def test_inverse_batch_rejects_slow_modulus():
     eng.close()
     p.close()
     c.close()
+
+
+def test_every_large_split_in_one_batch(ctx):
+    """Large sizes whose engine splits end in a 3- or 5-stage pass or need
+    three passes (2^11 = 8+3, 2^13 = 8+5, 2^17 = 6+8+3, 2^19 = 8+8+3,
+    2^21 = 8+8+5) in one mixed launch: bit-exact against the oracle up to
+    2^17, and forward-then-inverse round trips for all."""
+    b = W.uneven_batch(seed=33, n_small=300, large=((11, 2), (13, 1), (17, 1), (19, 1), (21, 1)))
+    s = Setup(ctx, b)
+    s.engine.run_dev(s.jobs())
+    assert s.engine.status() == bn.OK
+    y = s.output()
+    for i in range(b.count):
+        o, logn = int(b.offsets[i]), int(b.logns[i])
+        if 11 <= logn <= 17:
+            n = 1 << logn
+            want = C.oracle_ntt(s.x[o:o + n], s.tables[logn], logn, form=1)
+            assert np.array_equal(y[o:o + n], want), f"job {i} (2^{logn})"
+    zs = DevBuf(ctx, b.total * 16)
+    offs = [16 * int(o) for o in b.offsets]
+    back = bn.Batch.jobs([s.dy.addr + o for o in offs], [zs.addr + o for o in offs],
+                         [s.plan_ids[int(n)] for n in b.logns])
+    s.engine.run_inverse_dev(back)
+    assert s.engine.status() == bn.OK
+    assert np.array_equal(zs.to_array(), s.x)
+    zs.free()
+    s.close()
