@@ -59,7 +59,7 @@ def parse():
                     help="fraction of the uneven batch (profiling captures of a smaller case)")
     ap.add_argument("--headline-only", action="store_true",
                     help="only the persistent-kernel step (for profiler launch lists)")
-    ap.add_argument("--only", choices=["uniform", "inverse", "blas"], default=None,
+    ap.add_argument("--only", choices=["uniform", "inverse", "blas", "serving"], default=None,
                     help="run one secondary benchmark alone (profiling captures)")
     ap.add_argument("--logn", type=int, default=10, help="size for --only uniform")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -252,6 +252,8 @@ def run_only(args, dist: Dist):
     if args.only in ("uniform", "inverse"):
         res = uniform_bench(args, ctx, stream, ctx.imad_peak(), sizes=[args.logn],
                             inverse=args.only == "inverse")
+    elif args.only == "serving":
+        res = serving_bench(args, ctx)
     else:
         res = blas_bench(args, ctx, stream, measured_peaks())
     return {"only": args.only, "result": res}, ctx

@@ -95,8 +95,28 @@ struct Slot {
   size_t dev_cap = 0;
   void* pinned = nullptr;  // the same, staged in pinned host memory
   size_t pinned_cap = 0;
+  // outgrown staging buffers, freed when the server is destroyed: cudaFree and
+  // cudaFreeHost wait for the whole device, which would stall the worker
+  // behind every launch in flight
+  std::vector<void*> old_dev, old_pinned;
   std::vector<PendingReq> reqs;
 };
+
+// Output bytes admitted into one launch (a single larger request is admitted
+// alone).  Bounds the work a request can wait behind in its own launch and
+// the size of a launch's schedule, so the staging buffers are sized once.
+constexpr size_t kLaunchBytes = (size_t)256 << 20;
+
+// Staging bytes of the schedule of a launch with at most `jobs` NTTs holding
+// at most `elems` elements: every pass of a transform of 2^11 or more
+// elements has 2^n / 2048 tiles, and a small-size tile holds one job or more.
+inline size_t schedule_bytes_bound(size_t jobs, size_t elems) {
+  auto r256 = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  const size_t large = std::min(jobs, elems >> 11);
+  const size_t items = jobs + kMaxPasses * (elems >> 11);
+  return r256((kCtlHeader + large * kMaxPasses) * 4) + r256(large * kMaxPasses * 4) +
+         r256(items * sizeof(WorkItem)) + r256(jobs * 4) + r256(jobs * sizeof(DevJob));
+}
 
 }  // namespace bntt
 
@@ -148,13 +168,19 @@ static int launch_slot(bntt_server* s, Slot& slot) {
     auto r256 = [](size_t v) { return (v + 255) & ~(size_t)255; };
     const size_t o_pt = r256(cb), o_it = r256(o_pt + pb), o_or = r256(o_it + ib),
                  o_jb = r256(o_or + ob), need = r256(o_jb + jb);
-    if (slot.pinned_cap < need) {
-      if (slot.pinned) cudaFreeHost(slot.pinned);
-      slot.pinned = nullptr;
-      BNTT_CK(cudaMallocHost(&slot.pinned, need * 2));
-      slot.pinned_cap = need * 2;
+    if (slot.pinned_cap < need || slot.dev_cap < need) {  // not reached within kLaunchBytes
+      void *h = nullptr, *d = nullptr;
+      BNTT_CK(cudaMallocHost(&h, need * 2));
+      if (int rc = ctx_alloc(c, &d, need * 2)) {
+        cudaFreeHost(h);
+        return rc;
+      }
+      if (slot.pinned) slot.old_pinned.push_back(slot.pinned);
+      if (slot.dev) slot.old_dev.push_back(slot.dev);
+      slot.pinned = h;
+      slot.dev = d;
+      slot.pinned_cap = slot.dev_cap = need * 2;
     }
-    if (int rc = grow(c, &slot.dev, &slot.dev_cap, need * 2)) return rc;
     char* h = static_cast<char*>(slot.pinned);
     memset(h, 0, cb);  // control words start at zero
     memcpy(h + o_pt, sc.pass_tiles.data(), pb);
@@ -227,8 +253,10 @@ static void worker_main(bntt_server* s) {
       {
         std::lock_guard<std::mutex> g(s->mu);
         const double t = s->now();
+        size_t launch_bytes = 0;
         while (!s->pending.empty() && free_slot->reqs.size() < s->cfg.max_batch) {
           PendingReq& head = s->pending.front();
+          if (!free_slot->reqs.empty() && launch_bytes + head.bytes > kLaunchBytes) break;
           void* y = s->arena.alloc(head.bytes);
           if (!y) {  // wait for memory: keep arrival order
             s->admission_waits++;
@@ -236,6 +264,7 @@ static void worker_main(bntt_server* s) {
           }
           head.y = y;
           head.t_admit = t;
+          launch_bytes += head.bytes;
           free_slot->reqs.push_back(head);
           s->pending.pop_front();
         }
@@ -303,10 +332,31 @@ int bntt_server_create(bntt_ctx* c, bntt_server** out, bntt_plan* const* plans, 
   bool fast = false;
   s->blas_mp = make_params(*blas_modulus, &fast);
   s->blas_fast = arith_fast(c, fast);
+  // staging for the largest schedule one launch can have: kLaunchBytes of
+  // outputs, or one transform of the largest plan
+  unsigned max_log = 0;
+  for (const bntt_plan* p : s->engine->plans) max_log = std::max(max_log, p->log2n);
+  const size_t stage = schedule_bytes_bound(s->cfg.max_batch, std::max(kLaunchBytes / 16, (size_t)1 << max_log));
   s->slots.resize(s->cfg.slots);
   for (Slot& slot : s->slots) {
     cudaStreamCreateWithFlags(&slot.stream, cudaStreamNonBlocking);
     cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming);
+    if (!rc && cudaMallocHost(&slot.pinned, stage) == cudaSuccess) slot.pinned_cap = stage;
+    else if (!rc) rc = cuda_error(cudaErrorMemoryAllocation, "cudaMallocHost of the launch staging");
+    if (!rc) rc = ctx_alloc(c, &slot.dev, stage);
+    if (!rc) slot.dev_cap = stage;
+  }
+  if (rc) {
+    for (Slot& slot : s->slots) {
+      if (slot.dev) ctx_free(c, slot.dev);
+      if (slot.pinned) cudaFreeHost(slot.pinned);
+      cudaStreamDestroy(slot.stream);
+      cudaEventDestroy(slot.done);
+    }
+    ctx_free(c, s->arena_mem);
+    bntt_batch_destroy(s->engine);
+    delete s;
+    return rc;
   }
   s->t0 = std::chrono::steady_clock::now();
   s->worker = std::thread(worker_main, s);
@@ -326,6 +376,8 @@ int bntt_server_destroy(bntt_server* s) {
     free_schedule(s->ctx, slot.sched);
     if (slot.dev) ctx_free(s->ctx, slot.dev);
     if (slot.pinned) cudaFreeHost(slot.pinned);
+    for (void* p : slot.old_dev) ctx_free(s->ctx, p);
+    for (void* p : slot.old_pinned) cudaFreeHost(p);
     cudaStreamDestroy(slot.stream);
     cudaEventDestroy(slot.done);
   }

@@ -145,3 +145,29 @@ def test_replay_completes_every_request(serial):
     assert np.all(lat > 0) and np.all(np.isfinite(lat))
     assert wall >= arr[len(reqs) - 1].t_arrive
     fx.close()
+
+
+def test_launch_output_cap():
+    # one launch admits at most 256 MiB of outputs: six 128 MiB vvmuls take at
+    # least three launches; a 512 MiB request larger than the cap runs alone
+    fx = Fixture(slots=1)
+    ln = 1 << 23
+    a = C.uniform_pairs(71, ln, C.Q_BLAS)
+    b = C.uniform_pairs(72, ln, C.Q_BLAS)
+    da, db = fx.dev(a), fx.dev(b)
+    big = np.concatenate([a, a, a, a])
+    bigb = np.concatenate([b, b, b, b])
+    dba, dbb = fx.dev(big), fx.dev(bigb)
+    reqs = [bn.RequestC(bn.REQ_VVMUL, 0, ln, da.addr, db.addr, bn.U128.of(0), i, 0.0) for i in range(6)]
+    reqs.append(bn.RequestC(bn.REQ_VVMUL, 0, 4 * ln, dba.addr, dbb.addr, bn.U128.of(0), 6, 0.0))
+    outs = run_mix(fx, reqs)
+    head = 1 << 12
+    want = C.oracle_blas("vvmul", a[:head], b[:head], C.Q_BLAS, C.MU_BLAS, 0)
+    for i in range(6):
+        assert np.array_equal(outs[i], outs[0])
+    assert np.array_equal(outs[0][:head], want)
+    assert np.array_equal(outs[6][3 * ln:3 * ln + head], want)
+    st = fx.srv.stats()
+    assert st["launches"] >= 4
+    assert st["completed"] == 7
+    fx.close()
