@@ -54,6 +54,8 @@ struct bntt_batch {
   std::vector<size_t> dev_off;       // byte offset of each job in the region
   void* region = nullptr;
   size_t region_cap = 0;
+  uint32_t* group_err = nullptr;     // pinned copies of the groups' error words
+  size_t group_err_cap = 0;
   size_t last_launches = 0;
   // fault injection for tests of the failure path (bntt_batch_inject_wait_timeout)
   uint32_t inject_polls = 0;

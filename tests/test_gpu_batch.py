@@ -357,3 +357,24 @@ def test_every_large_split_in_one_batch(ctx):
     assert np.array_equal(zs.to_array(), s.x)
     zs.free()
     s.close()
+
+
+def test_run_host_reports_timeout_and_recovers(ctx):
+    """The host-buffer pipeline's failure path: an injected run whose waits
+    can never be satisfied returns BNTT_ETIMEOUT from bntt_batch_run_host
+    itself (every group's error word is read), and the next run is correct."""
+    b = W.uneven_batch(seed=12, n_small=300, large=((12, 2), (16, 1)))
+    s = Setup(ctx, b)
+    y = np.zeros_like(s.x)
+    xs = [s.x.ctypes.data + 16 * int(o) for o in b.offsets]
+    ys = [y.ctypes.data + 16 * int(o) for o in b.offsets]
+    jobs = bn.Batch.jobs(xs, ys, [s.plan_ids[int(n)] for n in b.logns])
+    bn.check(bn.lib().bntt_batch_inject_wait_timeout(s.engine.handle, 2000))
+    with pytest.raises(bn.BnttError) as e:
+        s.engine.run_host(jobs)
+    assert e.value.status == bn.ETIMEOUT
+    s.engine.run_host(jobs)
+    assert np.array_equal(y, s.expected())
+    s.engine.run_host(jobs)             # cached schedules
+    assert np.array_equal(y, s.expected())
+    s.close()
