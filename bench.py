@@ -428,21 +428,33 @@ def e2e_uneven(args, dist, ctx, engine, batch, pid) -> dict:
     hjobs = bn.Batch.jobs([xh.data_ptr() + int(o) for o in offs],
                           [yh.data_ptr() + int(o) for o in offs], [pid[int(n)] for n in batch.logns])
     steps = max(3, min(args.steps, 10))
-    for _ in range(max(1, min(args.warmup, 3))):
-        engine.run_host(hjobs)
-    dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        engine.run_host(hjobs)
-    dt = (time.perf_counter() - t0) / steps
-    dt = dist.max(dt)
+
+    def timed(queued: bool) -> float:
+        # queued: every step is one bntt_batch_run_host_async call, the steps
+        # back to back and one bntt_batch_sync at the end (a stream of
+        # batches); otherwise one synchronous bntt_batch_run_host per step
+        for _ in range(max(1, min(args.warmup, 3))):
+            engine.run_host_async(hjobs) if queued else engine.run_host(hjobs)
+        engine.sync()
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            engine.run_host_async(hjobs) if queued else engine.run_host(hjobs)
+        engine.sync()
+        return dist.max((time.perf_counter() - t0) / steps)
+
+    dt = timed(True)
+    dt_sync = timed(False)
     nbytes = batch.total * 16
     link = pcie_both_ways(xh, yh)
     del xh, yh
     return {"value": batch.count * dist.world / dt, "unit": UNIT, "h2d_bytes_per_step": nbytes,
             "d2h_bytes_per_step": nbytes, "ms_per_step": dt * 1e3, "steps": steps,
-            "api": "bntt_batch_run_host (pinned host buffers; pipelined copies)",
+            "api": "bntt_batch_run_host_async per step, back to back, then bntt_batch_sync "
+                   "(pinned host buffers; every step copies all inputs in and all outputs out)",
+            "one_call_at_a_time": {"value": batch.count * dist.world / dt_sync, "ms_per_step": dt_sync * 1e3,
+                                   "api": "bntt_batch_run_host (synchronous) per step"},
             "pcie_gbs_each_way": nbytes / dt / 1e9,
             "pcie_peak_gbs_each_way": link,
             "pcie_frac": (nbytes / dt / 1e9) / link if link else None,

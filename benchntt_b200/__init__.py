@@ -134,6 +134,8 @@ _SIGS = [
     ("bntt_batch_destroy", _I, [_P]),
     ("bntt_batch_run_dev", _I, [_P, ctypes.POINTER(JobC), _S]),
     ("bntt_batch_run_host", _I, [_P, ctypes.POINTER(JobC), _S]),
+    ("bntt_batch_run_host_async", _I, [_P, ctypes.POINTER(JobC), _S]),
+    ("bntt_batch_sync", _I, [_P]),
     ("bntt_batch_run_percall_dev", _I, [_P, ctypes.POINTER(JobC), _S]),
     ("bntt_batch_run_dev_noalloc", _I, [_P, ctypes.POINTER(JobC), _S]),
     ("bntt_batch_status", _I, [_P]),
@@ -419,6 +421,13 @@ class Batch:
 
     def run_host(self, jobs) -> None:
         check(lib().bntt_batch_run_host(self._h, jobs, len(jobs)))
+
+    def run_host_async(self, jobs) -> None:
+        """Queue a host-buffer run; buffers stay untouched until sync()."""
+        check(lib().bntt_batch_run_host_async(self._h, jobs, len(jobs)))
+
+    def sync(self) -> None:
+        check(lib().bntt_batch_sync(self._h))
 
     def run_inverse_dev(self, jobs) -> None:
         """Inverse transforms of the jobs (job.x -> job.y) in one launch."""

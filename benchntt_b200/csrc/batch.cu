@@ -154,9 +154,11 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
 }
 
 // Copies the schedule to the device and captures [memset control words,
-// kernel] into a graph on `stream`.
+// kernel] into a graph on `stream`.  sticky_err: the graph leaves the error
+// word alone (it is cleared here and by whoever reads it), so errors of
+// several replays accumulate until they are read.
 static int upload_and_capture(bntt_batch* b, Schedule& sc, cudaStream_t stream,
-                              bool inverse = false) {
+                              bool inverse = false, bool sticky_err = false) {
   bntt_ctx* c = b->ctx;
   const size_t jb = sc.djobs.size() * sizeof(DevJob), ob = sc.order.size() * 4,
                ib = sc.items.size() * sizeof(WorkItem), cb = (kCtlHeader + sc.nslots * kMaxPasses) * 4,
@@ -175,6 +177,7 @@ static int upload_and_capture(bntt_batch* b, Schedule& sc, cudaStream_t stream,
       for (uint32_t& t : tiles) t += 1;
     BNTT_CK(cudaMemcpyAsync(sc.d_pass_tiles, tiles.data(), pb, cudaMemcpyHostToDevice, stream));
   }
+  if (sticky_err) BNTT_CK(cudaMemsetAsync(sc.d_ctl, 0, cb, stream));
   BNTT_CK(cudaStreamSynchronize(stream));
   if (sc.exec) {
     cudaGraphExecDestroy(sc.exec);
@@ -209,7 +212,13 @@ static int upload_and_capture(bntt_batch* b, Schedule& sc, cudaStream_t stream,
   void* args[] = {&ba, &mp, &layout, &scales};  // the forward kernel takes the first three
   cudaGraph_t graph = nullptr;
   BNTT_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t e1 = cudaMemsetAsync(sc.d_ctl, 0, cb, stream);
+  cudaError_t e1;
+  if (!sticky_err) {
+    e1 = cudaMemsetAsync(sc.d_ctl, 0, cb, stream);
+  } else {  // ctl[0] (queue head) and ctl[2..] (pass counters), not ctl[1]
+    e1 = cudaMemsetAsync(sc.d_ctl, 0, 4, stream);
+    if (e1 == cudaSuccess && cb > 8) e1 = cudaMemsetAsync(static_cast<char*>(sc.d_ctl) + 8, 0, cb - 8, stream);
+  }
   cudaError_t e2 = cudaLaunchKernel(fn, dim3(sc.grid), dim3(kBatchThreads), args, smem, stream);
   cudaError_t e3 = cudaStreamEndCapture(stream, &graph);
   if (e1 != cudaSuccess) return cuda_error(e1, "cudaMemsetAsync(capture)");
@@ -280,6 +289,7 @@ int bntt_batch_destroy(bntt_batch* b) {
   for (Schedule& s : b->groups) free_schedule(c, s);
   if (b->region) ctx_free(c, b->region);
   if (b->group_err) cudaFreeHost(b->group_err);
+  for (cudaEvent_t e : b->group_out) cudaEventDestroy(e);
   delete b;
   return BNTT_OK;
 }
@@ -337,13 +347,37 @@ int bntt_batch_status(bntt_batch* b) {
 
 size_t bntt_batch_last_launches(bntt_batch* b) { return b ? b->last_launches : 0; }
 
+// Reads and clears the host groups' error words (the host pipeline's graphs
+// leave them sticky); every host-run stream must be idle.
+static int host_groups_status(bntt_batch* b) {
+  bntt_ctx* c = b->ctx;
+  cudaStream_t s = c->copy_stream[1];
+  const size_t ng = b->groups.size();
+  for (size_t g = 0; g < ng; ++g) {
+    b->group_err[g] = 0;
+    if (!b->groups[g].d_ctl) continue;
+    uint32_t* w = static_cast<uint32_t*>(b->groups[g].d_ctl) + 1;
+    BNTT_CK(cudaMemcpyAsync(&b->group_err[g], w, 4, cudaMemcpyDeviceToHost, s));
+    BNTT_CK(cudaMemsetAsync(w, 0, 4, s));
+  }
+  BNTT_CK(cudaStreamSynchronize(s));
+  bool err = b->host_err_pending;
+  b->host_err_pending = false;
+  for (size_t g = 0; g < ng; ++g) err |= b->group_err[g] != 0;
+  if (err) return set_error(BNTT_ETIMEOUT, "a pass of a large transform waited too long for its predecessor");
+  return BNTT_OK;
+}
+
 // Host buffers: jobs are packed into one device region (in place), split into
 // groups of about 1/16 of the bytes each.  Group g's inputs go up on one copy
 // stream, its graph runs on the context stream, its outputs come back on the
 // other copy stream, so transfers of neighbouring groups overlap each other
 // and the kernels.  Host copies of jobs adjacent in host memory are merged.
-// Schedules and graphs are cached while the job list stays the same.
-int bntt_batch_run_host(bntt_batch* b, const bntt_job* jobs, size_t count) {
+// Schedules and graphs are cached while the job list stays the same.  A run
+// returns once it is queued: the next run's input copy of group g waits only
+// for this run's output copy of group g, so back-to-back runs keep both copy
+// directions busy across the boundary between runs.
+int bntt_batch_run_host_async(bntt_batch* b, const bntt_job* jobs, size_t count) {
   BNTT_REQUIRE(b && (jobs || count == 0), "NULL argument");
   bntt_ctx* c = b->ctx;
   if (int rc = ctx_use_device(c)) return rc;
@@ -359,6 +393,17 @@ int bntt_batch_run_host(bntt_batch* b, const bntt_job* jobs, size_t count) {
   }
   auto bytes_of = [&](size_t i) { return (size_t)16 << b->plans[jobs[i].plan]->log2n; };
   if (!same) {
+    // earlier runs may still use the region and the groups' schedules: let
+    // them finish and keep their status for the next bntt_batch_sync
+    BNTT_CK(cudaStreamSynchronize(s_in));
+    BNTT_CK(cudaStreamSynchronize(s_run));
+    BNTT_CK(cudaStreamSynchronize(s_out));
+    if (b->host_inflight) {
+      const int rc = host_groups_status(b);
+      b->host_err_pending = rc == BNTT_ETIMEOUT;
+      if (rc && rc != BNTT_ETIMEOUT) return rc;
+      b->host_inflight = false;
+    }
     b->host_last_jobs.clear();
     size_t total = 0;
     b->dev_off.assign(count, 0);
@@ -394,7 +439,7 @@ int bntt_batch_run_host(bntt_batch* b, const bntt_job* jobs, size_t count) {
     for (size_t g = 0; g < ng; ++g) {
       const size_t f = b->group_first[g], e = b->group_first[g + 1];
       if (int rc = build_schedule(b, b->groups[g], dj.data() + f, e - f)) return rc;
-      if (int rc = upload_and_capture(b, b->groups[g], s_run)) return rc;
+      if (int rc = upload_and_capture(b, b->groups[g], s_run, false, true)) return rc;
     }
     if (b->group_err_cap < ng) {
       if (b->group_err) cudaFreeHost(b->group_err);
@@ -403,6 +448,11 @@ int bntt_batch_run_host(bntt_batch* b, const bntt_job* jobs, size_t count) {
       BNTT_CK(cudaMallocHost(&b->group_err, ng * sizeof(uint32_t)));
       b->group_err_cap = ng;
     }
+    // a fresh event per group: "group g's output copy of the latest run"
+    for (cudaEvent_t e : b->group_out) cudaEventDestroy(e);
+    b->group_out.assign(ng, nullptr);
+    for (cudaEvent_t& e : b->group_out) BNTT_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->group_out_recorded = false;
     if (!inject) b->host_last_jobs.assign(jobs, jobs + count);
   }
   b->inject_polls = 0;  // an injected fault lasts one run
@@ -414,6 +464,8 @@ int bntt_batch_run_host(bntt_batch* b, const bntt_job* jobs, size_t count) {
   const size_t ng = b->groups.size();
   for (size_t g = 0; g < ng; ++g) {
     const size_t f = b->group_first[g], e = b->group_first[g + 1];
+    // the previous run's output copy of this group has left the region
+    if (b->group_out_recorded) BNTT_CK(cudaStreamWaitEvent(s_in, b->group_out[g], 0));
     for (size_t i = f; i < e;) {  // merged input copies
       size_t j = i + 1, run = bytes_of(i);
       while (j < e && static_cast<const char*>(jobs[j].x) == static_cast<const char*>(jobs[i].x) + run) {
@@ -438,22 +490,28 @@ int bntt_batch_run_host(bntt_batch* b, const bntt_job* jobs, size_t count) {
       BNTT_CK(cudaMemcpyAsync(jobs[i].y, region + b->dev_off[i], run, cudaMemcpyDeviceToHost, s_out));
       i = j;
     }
+    BNTT_CK(cudaEventRecord(b->group_out[g], s_out));
   }
-  // error words: queued behind the last output copy, which follows every
-  // group's kernel, instead of one synchronous read per group
-  for (size_t g = 0; g < ng; ++g) {
-    b->group_err[g] = 0;
-    if (b->groups[g].d_ctl)
-      BNTT_CK(cudaMemcpyAsync(&b->group_err[g], static_cast<uint32_t*>(b->groups[g].d_ctl) + 1, 4,
-                              cudaMemcpyDeviceToHost, s_out));
-  }
-  BNTT_CK(cudaStreamSynchronize(s_in));
-  BNTT_CK(cudaStreamSynchronize(s_run));
-  BNTT_CK(cudaStreamSynchronize(s_out));
-  for (size_t g = 0; g < ng; ++g)
-    if (b->group_err[g])
-      return set_error(BNTT_ETIMEOUT, "a pass of a large transform waited too long for its predecessor");
+  b->group_out_recorded = true;
+  b->host_inflight = true;
   return BNTT_OK;
+}
+
+int bntt_batch_sync(bntt_batch* b) {
+  BNTT_REQUIRE(b, "NULL batch");
+  bntt_ctx* c = b->ctx;
+  if (int rc = ctx_use_device(c)) return rc;
+  BNTT_CK(cudaStreamSynchronize(c->copy_stream[0]));
+  BNTT_CK(cudaStreamSynchronize(c->stream));
+  BNTT_CK(cudaStreamSynchronize(c->copy_stream[1]));
+  if (!b->host_inflight && !b->host_err_pending) return BNTT_OK;
+  b->host_inflight = false;
+  return host_groups_status(b);
+}
+
+int bntt_batch_run_host(bntt_batch* b, const bntt_job* jobs, size_t count) {
+  if (int rc = bntt_batch_run_host_async(b, jobs, count)) return rc;
+  return bntt_batch_sync(b);
 }
 
 }  // extern "C"

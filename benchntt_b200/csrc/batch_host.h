@@ -56,6 +56,10 @@ struct bntt_batch {
   size_t region_cap = 0;
   uint32_t* group_err = nullptr;     // pinned copies of the groups' error words
   size_t group_err_cap = 0;
+  std::vector<cudaEvent_t> group_out;  // per group: its output copy of the latest run
+  bool group_out_recorded = false;
+  bool host_inflight = false;        // host runs not yet passed to bntt_batch_sync
+  bool host_err_pending = false;     // an error of runs finished before a rebuild
   size_t last_launches = 0;
   // fault injection for tests of the failure path (bntt_batch_inject_wait_timeout)
   uint32_t inject_polls = 0;

@@ -215,6 +215,15 @@ int bntt_batch_destroy(bntt_batch *batch);
 int bntt_batch_run_dev(bntt_batch *batch, const bntt_job *jobs, size_t count);
 /* Host pointers: inputs copied in, batch run, outputs copied back. */
 int bntt_batch_run_host(bntt_batch *batch, const bntt_job *jobs, size_t count);
+/* The same, returning once the copies and launches are queued.  The host
+ * buffers must stay valid, the inputs unchanged and the outputs unread until
+ * bntt_batch_sync.  Back-to-back calls overlap: one call's output copies run
+ * under the next call's input copies.  No counterpart in the reference (its
+ * functions are synchronous, src/ntt_scalar.c:582). */
+int bntt_batch_run_host_async(bntt_batch *batch, const bntt_job *jobs, size_t count);
+/* Waits for every bntt_batch_run_host_async call so far; BNTT_ETIMEOUT if a
+ * device-side wait of any of them gave up. */
+int bntt_batch_sync(bntt_batch *batch);
 /* The same jobs, each launched on its own (one launch per transform of at
  * most 1024 points, one per HBM pass above): the per-call path the
  * persistent kernel is compared with.  Device pointers, asynchronous. */

@@ -378,3 +378,51 @@ def test_run_host_reports_timeout_and_recovers(ctx):
     s.engine.run_host(jobs)             # cached schedules
     assert np.array_equal(y, s.expected())
     s.close()
+
+
+def test_run_host_async_chained_in_place(ctx):
+    """Back-to-back asynchronous host runs are ordered group by group: with
+    in-place jobs (x == y on the host) three queued runs give ntt(ntt(ntt(x)))
+    for every job, which holds only if each run's input copy of a group waits
+    for the previous run's output copy of it."""
+    b = W.uneven_batch(seed=13, n_small=2000, large=((16, 3), (20, 1)))
+    s = Setup(ctx, b)
+    buf = s.x.copy()
+    ptrs = [buf.ctypes.data + 16 * int(o) for o in b.offsets]
+    jobs = bn.Batch.jobs(ptrs, ptrs, [s.plan_ids[int(n)] for n in b.logns])
+    for _ in range(3):
+        s.engine.run_host_async(jobs)
+    s.engine.sync()
+    ns = [int(n) for n in b.logns]
+    ts = [s.tables[n] for n in ns]
+    want = [s.x[o:o + (1 << n)] for o, n in zip(b.offsets, ns)]
+    for _ in range(3):
+        want = C.oracle_ntt_jobs(want, ts, ns, threads=8)
+    assert np.array_equal(buf, np.concatenate(want))
+    s.close()
+
+
+def test_run_host_async_reports_timeout_at_sync(ctx):
+    """An injected wait timeout in a queued host run is reported by
+    bntt_batch_sync, also when a later run with another job list had to
+    rebuild the schedules first; the runs after it are correct."""
+    b = W.uneven_batch(seed=14, n_small=300, large=((12, 2), (16, 1)))
+    s = Setup(ctx, b)
+    y = np.zeros_like(s.x)
+    xs = [s.x.ctypes.data + 16 * int(o) for o in b.offsets]
+    ys = [y.ctypes.data + 16 * int(o) for o in b.offsets]
+    ids = [s.plan_ids[int(n)] for n in b.logns]
+    jobs = bn.Batch.jobs(xs, ys, ids)
+    part = bn.Batch.jobs(xs[:100], ys[:100], ids[:100])
+    bn.check(bn.lib().bntt_batch_inject_wait_timeout(s.engine.handle, 2000))
+    s.engine.run_host_async(jobs)
+    s.engine.run_host_async(part)        # another job list: rebuild after the faulty run
+    with pytest.raises(bn.BnttError) as e:
+        s.engine.sync()
+    assert e.value.status == bn.ETIMEOUT
+    s.engine.sync()                       # reported once
+    s.engine.run_host_async(jobs)
+    s.engine.run_host_async(jobs)
+    s.engine.sync()
+    assert np.array_equal(y, s.expected())
+    s.close()
