@@ -194,3 +194,56 @@ def test_budget_rejects_plan(ctx):
         bn.Plan(c, 10, C.Q_NTT, C.MU_NTT, C.uniform_pairs(1, 1024, C.Q_NTT))
     assert e.value.status == bn.EBUDGET
     c.close()
+
+
+def rare_sum_inputs(logn, batch, q=C.Q_NTT):
+    """Transforms whose stage-0 pairs (j, j + N/2) sum to addmod's rare cases
+    under an all-ones table: sums in (q, 2^124), sums equal to q and 2^124,
+    sums above 2^124 whose low 64 bits equal q's (the borrow quirk), other
+    sums with limb 1 = 0xFFFFFFFF, and ordinary sums.  Each sum s is split as
+    x = s - s // 2, y = s // 2, both at most q."""
+    k = (1 << 124) - q
+    rng = np.random.default_rng(logn)
+    sums = [q + 1, q + 2, q + k - 1, q, q - 1, 1 << 124, (1 << 124) + 1, (1 << 124) - 1]
+    sums += [q + j * (1 << 64) for j in (1, 2, 3, 1 << 40, (q >> 64) - 1)]
+    for _ in range(24):
+        hi = int(rng.integers(0, 1 << 61)) % (q >> 64)
+        lo = (0xFFFFFFFF << 32) | int(rng.integers(0, 1 << 32))
+        s = (hi << 64) | lo
+        sums.append(s if s < 2 * q else s - q)
+    sums += [int(v) for v in C.from_pairs(C.uniform_pairs(77 + logn, 32, 2 * q))]
+    half = 1 << (logn - 1)
+    xs = np.empty((batch << logn, 2), dtype=np.uint64)
+    for t in range(batch):
+        lo_half, hi_half = [], []
+        for i in range(half):
+            s = sums[(t * half + i) % len(sums)]
+            hi_half.append(s // 2)
+            lo_half.append(s - s // 2)
+        xs[t << logn:(t + 1) << logn] = C.to_pairs(lo_half + hi_half)
+    return xs
+
+
+@pytest.mark.parametrize("logn,batch", [(1, 70), (4, 9), (10, 2), (12, 1), (16, 1)])
+def test_addmod_rare_sums(ctx, logn, batch):
+    """The fast addmod's exceptional sums (one in 2^32 for uniform data, so
+    constructed here) through the plan kernels and the persistent batch
+    kernel, against the oracle."""
+    n = 1 << logn
+    x = rare_sum_inputs(logn, batch)
+    t = C.to_pairs([1] * n)
+    want = C.oracle_ntt(x, t, logn)
+    assert np.array_equal(run_dev(ctx, x, t, logn), want)
+    plan = bn.Plan(ctx, logn, C.Q_NTT, C.MU_NTT, t)
+    engine = bn.Batch(ctx, [plan])
+    dx = DevBuf.from_array(ctx, x)
+    dy = DevBuf(ctx, x.nbytes)
+    jobs = bn.Batch.jobs([dx.addr + 16 * n * i for i in range(batch)],
+                         [dy.addr + 16 * n * i for i in range(batch)], [0] * batch)
+    engine.run_dev(jobs)
+    assert engine.status() == bn.OK
+    assert np.array_equal(dy.to_array(x.shape[0]), want)
+    dx.free()
+    dy.free()
+    engine.close()
+    plan.close()
