@@ -206,10 +206,7 @@ static int upload_and_capture(bntt_batch* b, Schedule& sc, cudaStream_t stream,
   ba.wait_polls = b->inject_polls ? b->inject_polls : kWaitPolls;
   ModParams mp = b->mp;
   int layout = b->layout;
-  InvScales scales{};
-  for (const bntt_plan* p : b->plans)
-    scales.ninv[p->log2n] = make_uint4(p->ninv.w[0], p->ninv.w[1], p->ninv.w[2], p->ninv.w[3]);
-  void* args[] = {&ba, &mp, &layout, &scales};  // the forward kernel takes the first three
+  void* args[] = {&ba, &mp, &layout};
   cudaGraph_t graph = nullptr;
   BNTT_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t e1;

@@ -114,11 +114,6 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
   return v;
 }
 
-// N^-1 mod q for each log2 N (limb order), for the inverse batch kernel.
-struct InvScales {
-  uint4 ninv[25];
-};
-
 struct BatchArgs {
   const WorkItem* items;
   uint32_t nitems;

@@ -3,7 +3,8 @@
 // item runs the inverse network (ntt_engine.cuh in inverse mode, stages last
 // to first with the plans' inverse tables), the passes of a large job run
 // from the last to the first, and whatever finishes a transform -- a small
-// tile, or pass 0 of a large job -- multiplies by N^-1 as it stores.
+// tile, or pass 0 of a large job -- multiplies by N^-1 as it stores, read
+// from entry 0 of the job's inverse table (no stage uses that entry).
 // Fast moduli only, like the plans' inverse.
 #include "batch_dev.cuh"
 
@@ -14,8 +15,7 @@ namespace {
 // 2^1, 2^2: one thread per transform.
 template <int M>
 __device__ __noinline__ void run_item_tiny_inv(const WorkItem& it, const BatchArgs& ba,
-                                               const ModParams& mp, int layout,
-                                               const InvScales& sc, int* s_flag) {
+                                               const ModParams& mp, int layout, int* s_flag) {
   SubRef sr;
   if (!item_subref<true>(it, ba, M, threadIdx.x, s_flag, &sr)) return;
   if (!sr.valid) return;
@@ -33,15 +33,14 @@ __device__ __noinline__ void run_item_tiny_inv(const WorkItem& it, const BatchAr
       gs_butterfly<ArithFast>(v[i], v[i + half], U128{{tv.x, tv.y, tv.z, tv.w}}, mp);
     }
   }
-  const uint4 f = sc.ninv[M];
+  const uint4 f = __ldg(sr.tw);  // N^-1
   const U128 ninv = U128{{f.x, f.y, f.z, f.w}};
 #pragma unroll
   for (int i = 0; i < N; ++i) sr.y[i] = to_mem(ArithFast::mul(v[i], ninv, mp), layout);
 }
 
 __device__ __noinline__ void run_item_engine_inv(const WorkItem& it, const BatchArgs& ba, uint4* smem,
-                                                 const ModParams& mp, int layout,
-                                                 const InvScales& sc, int* s_flag) {
+                                                 const ModParams& mp, int layout, int* s_flag) {
   using E = NttEngine<3, ArithFast>;
   int m, map;
   shape_of(it.shape, &m, &map);
@@ -53,7 +52,7 @@ __device__ __noinline__ void run_item_engine_inv(const WorkItem& it, const Batch
   const bool finishes = it.kind == ITEM_SMALL || it.pass == 0;
   Epilogue ep;
   if (finishes) {
-    const uint4 f = sc.ninv[it.kind == ITEM_SMALL ? m : (int)ba.jobs[it.a].log2n];
+    const uint4 f = __ldg(it.kind == ITEM_SMALL ? sr.tw : ba.jobs[it.a].tw);  // N^-1
     ep.scale = U128{{f.x, f.y, f.z, f.w}};
     ep.has_scale = 1;
   }
@@ -64,7 +63,7 @@ __device__ __noinline__ void run_item_engine_inv(const WorkItem& it, const Batch
 
 template <int MINB>
 __global__ void __launch_bounds__(kBatchThreads, MINB)
-    k_batch_inv(BatchArgs ba, ModParams mp, int layout, InvScales sc) {
+    k_batch_inv(BatchArgs ba, ModParams mp, int layout) {
   extern __shared__ uint4 smem[];
   __shared__ uint32_t s_item;
   __shared__ int s_flag;
@@ -74,9 +73,9 @@ __global__ void __launch_bounds__(kBatchThreads, MINB)
     const uint32_t i = s_item;
     if (i >= ba.nitems) break;
     const WorkItem it = ba.items[i];
-    if (it.shape == 0) run_item_tiny_inv<1>(it, ba, mp, layout, sc, &s_flag);
-    else if (it.shape == 1) run_item_tiny_inv<2>(it, ba, mp, layout, sc, &s_flag);
-    else run_item_engine_inv(it, ba, smem, mp, layout, sc, &s_flag);
+    if (it.shape == 0) run_item_tiny_inv<1>(it, ba, mp, layout, &s_flag);
+    else if (it.shape == 1) run_item_tiny_inv<2>(it, ba, mp, layout, &s_flag);
+    else run_item_engine_inv(it, ba, smem, mp, layout, &s_flag);
     __syncthreads();  // smem and s_item are reused by the next item
   }
 }

@@ -134,7 +134,8 @@ int engine_passes(bntt_plan* p, void* out, const void* in, size_t batch, const v
 // Inverse table (T[k]^-1, limb order) and N^-1, built once per plan: the
 // forward table comes back from the device and is inverted on the host with
 // one modular exponentiation and three multiplies per entry (batch
-// inversion).
+// inversion).  Entry 0, which no network stage reads, holds N^-1: the
+// inverse batch kernel takes each job's scale from its own table.
 int ensure_inverse(bntt_plan* p) {
   if (p->tw_inv) return BNTT_OK;
   const u128 q = to_u128(p->mod.q), mu = to_u128(p->mod.mu);
@@ -162,7 +163,6 @@ int ensure_inverse(bntt_plan* p) {
   BNTT_REQUIRE(host_mulmod(inv, acc, q, mu) == 1,
                "the product of the twiddles has no inverse mod q (q is not prime)");
   std::vector<uint32_t> ti(4 * n, 0);
-  ti[0] = 1;  // entry 0 is never read
   for (size_t k = n - 1; k >= 1; --k) {
     const u128 ik = host_mulmod(inv, pre[k], q, mu);  // = T[k]^-1
     inv = host_mulmod(inv, entry(k), q, mu);
@@ -170,6 +170,7 @@ int ensure_inverse(bntt_plan* p) {
   }
   const u128 ninv = host_powmod((u128)n % q, q - 2, q, mu);
   BNTT_REQUIRE(host_mulmod(ninv, (u128)n % q, q, mu) == 1, "N has no inverse mod q");
+  for (int l = 0; l < 4; ++l) ti[l] = (uint32_t)(ninv >> (32 * l));
   void* d = nullptr;
   if (int rc = ctx_alloc(p->ctx, &d, n * 16)) return rc;
   cudaError_t e = cudaMemcpyAsync(d, ti.data(), n * 16, cudaMemcpyHostToDevice, p->ctx->stream);
