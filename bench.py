@@ -372,6 +372,8 @@ def run_ours(args, dist: Dist):
 
     # ------------------------------------------------------------ e2e (host)
     result["e2e"] = e2e_uneven(args, dist, ctx, engine, batch, pid)
+    # ------------------------------------------- a new job list every step
+    result["new_job_list_each_step"] = fresh_lists(args, ctx, stream, engine, jobs, batch, value)
     # ---------------------------------------------------------- per-call path
     result["per_call"] = per_call(args, dist, ctx, stream, engine, jobs, batch, value)
     # ----------------------------------------------------------------- BLAS
@@ -484,6 +486,33 @@ def pcie_both_ways(xh, yh) -> float:
     dt = (time.perf_counter() - t0) / 3
     del dx, dy
     return xh.numel() * 8 / dt / 1e9
+
+
+def fresh_lists(args, ctx, stream, engine, jobs, batch, batched_value) -> dict:
+    """The headline batch with the job list alternating between two orders
+    (the given one and its reverse), so every step is a job list the engine
+    did not run last: schedule built on the host, copied while the previous
+    launch runs, launched without a graph."""
+    import torch
+
+    import benchntt_b200 as bn
+    rev = (bn.JobC * len(jobs))(*reversed(list(jobs)))
+    lists = (jobs, rev)
+    for i in range(4):
+        engine.run_dev(lists[i % 2])
+    ctx.synchronize()
+    steps = max(10, min(args.steps, 40))
+    e0, e1 = cuda_events()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for i in range(steps):
+        engine.run_dev(lists[i % 2])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / steps
+    ms = e0.elapsed_time(e1) / steps
+    return {"value": batch.count / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "host_wall_ms_per_step": wall * 1e3, "vs_same_list": batch.count / (ms * 1e-3) / batched_value}
 
 
 def per_call(args, dist, ctx, stream, engine, jobs, batch, batched_value) -> dict:

@@ -58,11 +58,25 @@ int grow(bntt_ctx* c, void** p, size_t* cap, size_t bytes) {
 void free_schedule(bntt_ctx* c, Schedule& s) {
   if (s.exec) cudaGraphExecDestroy(s.exec);
   s.exec = nullptr;
-  for (void** p : {&s.d_jobs, &s.d_order, &s.d_items, &s.d_ctl, &s.d_pass_tiles}) {
-    if (*p) ctx_free(c, *p);
-    *p = nullptr;
+  for (cudaGraphExec_t e : s.retired) cudaGraphExecDestroy(e);
+  s.retired.clear();
+  for (int i = 0; i < 2; ++i) {
+    if (s.stage_done[i]) cudaEventSynchronize(s.stage_done[i]);
+    if (s.set_free[i]) cudaEventSynchronize(s.set_free[i]);
+    if (s.stage[i]) cudaFreeHost(s.stage[i]);
+    if (s.stage_done[i]) cudaEventDestroy(s.stage_done[i]);
+    if (s.set_free[i]) cudaEventDestroy(s.set_free[i]);
+    if (s.d_sched[i]) ctx_free(c, s.d_sched[i]);
+    s.stage[i] = s.d_sched[i] = nullptr;
+    s.stage_done[i] = s.set_free[i] = nullptr;
+    s.stage_cap[i] = s.d_sched_cap[i] = 0;
+    s.set_used[i] = false;
   }
-  s.d_jobs_cap = s.d_order_cap = s.d_items_cap = s.d_ctl_cap = s.d_pass_tiles_cap = 0;
+  if (s.set_ready) cudaEventDestroy(s.set_ready);
+  s.set_ready = nullptr;
+  if (s.d_ctl) ctx_free(c, s.d_ctl);
+  s.d_ctl = nullptr;
+  s.d_ctl_cap = 0;
 }
 
 const void* batch_kernel(bool fast) { return fast ? batch_kernel_fast_minb(g_batch_minb) : batch_kernel_ref(); }
@@ -153,36 +167,77 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
   return BNTT_OK;
 }
 
-// Copies the schedule to the device and captures [memset control words,
-// kernel] into a graph on `stream`.  sticky_err: the graph leaves the error
-// word alone (it is cleared here and by whoever reads it), so errors of
-// several replays accumulate until they are read.
-static int upload_and_capture(bntt_batch* b, Schedule& sc, cudaStream_t stream,
-                              bool inverse = false, bool sticky_err = false) {
+// Graphs of earlier job lists; the caller has synchronized `sc.stream`.
+static void destroy_retired(Schedule& sc) {
+  for (cudaGraphExec_t e : sc.retired) cudaGraphExecDestroy(e);
+  sc.retired.clear();
+}
+
+// Copies the schedule to the device and sizes its launch on `stream`.  The
+// copy goes through pinned staging into the device buffer that the previous
+// job list's launches do not read; with `copy_stream` it runs there, waiting
+// only for the last launch that read that buffer, so it overlaps the launches
+// in flight, and `stream` waits for it.  Without, it is queued on `stream`.
+// The previous list's graph is retired, not destroyed, since a replay of it
+// may still be running.  sticky_err: launches leave the error word alone (it
+// is cleared here and by whoever reads it), so errors of several launches
+// accumulate until they are read.
+static int upload(bntt_batch* b, Schedule& sc, cudaStream_t stream, bool inverse = false,
+                  bool sticky_err = false, cudaStream_t copy_stream = nullptr) {
   bntt_ctx* c = b->ctx;
   const size_t jb = sc.djobs.size() * sizeof(DevJob), ob = sc.order.size() * 4,
                ib = sc.items.size() * sizeof(WorkItem), cb = (kCtlHeader + sc.nslots * kMaxPasses) * 4,
                pb = sc.pass_tiles.size() * 4;
-  int rc;
-  if ((rc = grow(c, &sc.d_jobs, &sc.d_jobs_cap, jb)) || (rc = grow(c, &sc.d_order, &sc.d_order_cap, ob)) ||
-      (rc = grow(c, &sc.d_items, &sc.d_items_cap, ib)) || (rc = grow(c, &sc.d_ctl, &sc.d_ctl_cap, cb)) ||
-      (rc = grow(c, &sc.d_pass_tiles, &sc.d_pass_tiles_cap, pb)))
-    return rc;
-  if (jb) BNTT_CK(cudaMemcpyAsync(sc.d_jobs, sc.djobs.data(), jb, cudaMemcpyHostToDevice, stream));
-  if (ob) BNTT_CK(cudaMemcpyAsync(sc.d_order, sc.order.data(), ob, cudaMemcpyHostToDevice, stream));
-  if (ib) BNTT_CK(cudaMemcpyAsync(sc.d_items, sc.items.data(), ib, cudaMemcpyHostToDevice, stream));
-  if (pb) {
-    std::vector<uint32_t> tiles = sc.pass_tiles;
-    if (b->inject_polls)  // injected fault: every wait needs one tile more than exists
-      for (uint32_t& t : tiles) t += 1;
-    BNTT_CK(cudaMemcpyAsync(sc.d_pass_tiles, tiles.data(), pb, cudaMemcpyHostToDevice, stream));
-  }
-  if (sticky_err) BNTT_CK(cudaMemsetAsync(sc.d_ctl, 0, cb, stream));
-  BNTT_CK(cudaStreamSynchronize(stream));
+  auto r256 = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  const size_t o_ob = r256(jb), o_ib = o_ob + r256(ob), o_pb = o_ib + r256(ib), total = o_pb + r256(pb);
   if (sc.exec) {
-    cudaGraphExecDestroy(sc.exec);
+    sc.retired.push_back(sc.exec);
     sc.exec = nullptr;
   }
+  if (sc.retired.size() > 8) {  // bound the graphs kept alive
+    BNTT_CK(cudaStreamSynchronize(sc.stream ? sc.stream : stream));
+    destroy_retired(sc);
+  }
+  const int set = sc.cur ^ 1;
+  cudaStream_t cs = copy_stream ? copy_stream : stream;
+  if (int rc = grow(c, &sc.d_sched[set], &sc.d_sched_cap[set], total)) return rc;
+  if (int rc = grow(c, &sc.d_ctl, &sc.d_ctl_cap, cb)) return rc;
+  if (sc.set_used[set] && cs != stream) BNTT_CK(cudaStreamWaitEvent(cs, sc.set_free[set], 0));
+  const int si = sc.stage_next;
+  sc.stage_next ^= 1;
+  if (sc.stage_done[si]) BNTT_CK(cudaEventSynchronize(sc.stage_done[si]));
+  else BNTT_CK(cudaEventCreateWithFlags(&sc.stage_done[si], cudaEventDisableTiming));
+  if (sc.stage_cap[si] < total) {
+    if (sc.stage[si]) cudaFreeHost(sc.stage[si]);
+    sc.stage[si] = nullptr;
+    sc.stage_cap[si] = 0;
+    BNTT_CK(cudaMallocHost(&sc.stage[si], total + total / 2));
+    sc.stage_cap[si] = total + total / 2;
+  }
+  char* h = static_cast<char*>(sc.stage[si]);
+  if (jb) memcpy(h, sc.djobs.data(), jb);
+  if (ob) memcpy(h + o_ob, sc.order.data(), ob);
+  if (ib) memcpy(h + o_ib, sc.items.data(), ib);
+  if (pb) {
+    uint32_t* t = reinterpret_cast<uint32_t*>(h + o_pb);
+    memcpy(t, sc.pass_tiles.data(), pb);
+    if (b->inject_polls)  // injected fault: every wait needs one tile more than exists
+      for (size_t i = 0; i < sc.pass_tiles.size(); ++i) t[i] += 1;
+  }
+  char* d = static_cast<char*>(sc.d_sched[set]);
+  BNTT_CK(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, cs));
+  BNTT_CK(cudaEventRecord(sc.stage_done[si], cs));
+  if (cs != stream) {
+    if (!sc.set_ready) BNTT_CK(cudaEventCreateWithFlags(&sc.set_ready, cudaEventDisableTiming));
+    BNTT_CK(cudaEventRecord(sc.set_ready, cs));
+    BNTT_CK(cudaStreamWaitEvent(stream, sc.set_ready, 0));
+  }
+  sc.cur = set;
+  if (sticky_err) BNTT_CK(cudaMemsetAsync(sc.d_ctl, 0, cb, stream));
+  sc.stream = stream;
+  sc.inverse = inverse;
+  sc.sticky_err = sticky_err;
+  sc.grid = 0;
   if (sc.items.empty()) return BNTT_OK;
   const void* fn = inverse ? batch_kernel_inverse() : batch_kernel(b->fast);
   size_t smem = 0;
@@ -196,41 +251,69 @@ static int upload_and_capture(bntt_batch* b, Schedule& sc, cudaStream_t stream,
   if (bps < 1) return set_error(BNTT_ECUDA, "batch kernel does not fit on an SM (smem %zu)", smem);
   sc.grid = (int)std::min<size_t>((size_t)bps * c->sms, sc.items.size());
   sc.smem = smem;
-  BatchArgs ba;
-  ba.items = static_cast<const WorkItem*>(sc.d_items);
+  BatchArgs& ba = sc.args;
+  ba.items = reinterpret_cast<const WorkItem*>(d + o_ib);
   ba.nitems = (uint32_t)sc.items.size();
-  ba.jobs = static_cast<const DevJob*>(sc.d_jobs);
-  ba.order = static_cast<const uint32_t*>(sc.d_order);
+  ba.jobs = reinterpret_cast<const DevJob*>(d);
+  ba.order = reinterpret_cast<const uint32_t*>(d + o_ob);
   ba.ctl = static_cast<uint32_t*>(sc.d_ctl);
-  ba.pass_tiles = static_cast<const uint32_t*>(sc.d_pass_tiles);
+  ba.pass_tiles = reinterpret_cast<const uint32_t*>(d + o_pb);
   ba.wait_polls = b->inject_polls ? b->inject_polls : kWaitPolls;
-  ModParams mp = b->mp;
-  int layout = b->layout;
-  void* args[] = {&ba, &mp, &layout};
-  cudaGraph_t graph = nullptr;
-  BNTT_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t e1;
-  if (!sticky_err) {
-    e1 = cudaMemsetAsync(sc.d_ctl, 0, cb, stream);
-  } else {  // ctl[0] (queue head) and ctl[2..] (pass counters), not ctl[1]
-    e1 = cudaMemsetAsync(sc.d_ctl, 0, 4, stream);
-    if (e1 == cudaSuccess && cb > 8) e1 = cudaMemsetAsync(static_cast<char*>(sc.d_ctl) + 8, 0, cb - 8, stream);
-  }
-  cudaError_t e2 = cudaLaunchKernel(fn, dim3(sc.grid), dim3(kBatchThreads), args, smem, stream);
-  cudaError_t e3 = cudaStreamEndCapture(stream, &graph);
-  if (e1 != cudaSuccess) return cuda_error(e1, "cudaMemsetAsync(capture)");
-  if (e2 != cudaSuccess) return cuda_error(e2, "cudaLaunchKernel(capture)");
-  if (e3 != cudaSuccess) return cuda_error(e3, "cudaStreamEndCapture");
-  cudaError_t e4 = cudaGraphInstantiate(&sc.exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (e4 != cudaSuccess) return cuda_error(e4, "cudaGraphInstantiate");
-  sc.exec_stream = stream;
   return BNTT_OK;
 }
 
+// [clear the control words, kernel] of an uploaded schedule on `stream`.
+static cudaError_t enqueue_run(bntt_batch* b, Schedule& sc, cudaStream_t stream) {
+  const size_t cb = (kCtlHeader + sc.nslots * kMaxPasses) * 4;
+  cudaError_t e;
+  if (!sc.sticky_err) {
+    e = cudaMemsetAsync(sc.d_ctl, 0, cb, stream);
+  } else {  // ctl[0] (queue head) and ctl[2..] (pass counters), not ctl[1]
+    e = cudaMemsetAsync(sc.d_ctl, 0, 4, stream);
+    if (e == cudaSuccess && cb > 8) e = cudaMemsetAsync(static_cast<char*>(sc.d_ctl) + 8, 0, cb - 8, stream);
+  }
+  if (e != cudaSuccess) return e;
+  const void* fn = sc.inverse ? batch_kernel_inverse() : batch_kernel(b->fast);
+  BatchArgs ba = sc.args;
+  ModParams mp = b->mp;
+  int layout = b->layout;
+  void* args[] = {&ba, &mp, &layout};
+  return cudaLaunchKernel(fn, dim3(sc.grid), dim3(kBatchThreads), args, sc.smem, stream);
+}
+
+// Captures the schedule's launch into a graph for later replays.
+static int capture(bntt_batch* b, Schedule& sc) {
+  if (sc.exec || sc.grid == 0) return BNTT_OK;
+  cudaGraph_t graph = nullptr;
+  BNTT_CK(cudaStreamBeginCapture(sc.stream, cudaStreamCaptureModeThreadLocal));
+  const cudaError_t e1 = enqueue_run(b, sc, sc.stream);
+  const cudaError_t e2 = cudaStreamEndCapture(sc.stream, &graph);
+  if (e1 != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return cuda_error(e1, "batch launch (capture)");
+  }
+  if (e2 != cudaSuccess) return cuda_error(e2, "cudaStreamEndCapture");
+  const cudaError_t e3 = cudaGraphInstantiate(&sc.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e3 != cudaSuccess) {
+    sc.exec = nullptr;
+    return cuda_error(e3, "cudaGraphInstantiate");
+  }
+  return BNTT_OK;
+}
+
+// A replay of the captured graph, or the launch itself when there is none.
 static int launch_schedule(bntt_batch* b, Schedule& sc, cudaStream_t stream) {
-  if (!sc.exec) return BNTT_OK;
-  BNTT_CK(cudaGraphLaunch(sc.exec, stream));
+  if (sc.grid == 0) return BNTT_OK;
+  if (sc.exec) {
+    BNTT_CK(cudaGraphLaunch(sc.exec, stream));
+  } else {
+    const cudaError_t e = enqueue_run(b, sc, stream);
+    if (e != cudaSuccess) return cuda_error(e, "batch launch");
+  }
+  if (!sc.set_free[sc.cur]) BNTT_CK(cudaEventCreateWithFlags(&sc.set_free[sc.cur], cudaEventDisableTiming));
+  BNTT_CK(cudaEventRecord(sc.set_free[sc.cur], stream));
+  sc.set_used[sc.cur] = true;
   b->ctx->launches++;
   b->last_launches++;
   return BNTT_OK;
@@ -271,6 +354,10 @@ int bntt_batch_create(bntt_ctx* c, bntt_batch** out, bntt_plan* const* plans, si
     b->shapes.pass_contig[m] = batch_shape_for(m, MAP_CONTIG, 4);
     if (b->shapes.pass_contig[m] < 0) b->shapes.pass_contig[m] = batch_shape_for(m, MAP_CONTIG, 0);
   }
+  if (cudaError_t e = cudaStreamCreateWithFlags(&b->upload_stream, cudaStreamNonBlocking)) {
+    delete b;
+    return cuda_error(e, "cudaStreamCreateWithFlags");
+  }
   *out = b;
   return BNTT_OK;
 }
@@ -281,12 +368,14 @@ int bntt_batch_destroy(bntt_batch* b) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   for (int s = 0; s < 2; ++s) cudaStreamSynchronize(c->copy_stream[s]);
+  if (b->upload_stream) cudaStreamSynchronize(b->upload_stream);
   free_schedule(c, b->main);
   free_schedule(c, b->inv);
   for (Schedule& s : b->groups) free_schedule(c, s);
   if (b->region) ctx_free(c, b->region);
   if (b->group_err) cudaFreeHost(b->group_err);
   for (cudaEvent_t e : b->group_out) cudaEventDestroy(e);
+  if (b->upload_stream) cudaStreamDestroy(b->upload_stream);
   delete b;
   return BNTT_OK;
 }
@@ -297,13 +386,15 @@ int bntt_batch_run_dev(bntt_batch* b, const bntt_job* jobs, size_t count) {
   b->last_launches = 0;
   if (count == 0) return BNTT_OK;
   const bool inject = b->inject_polls != 0;
-  const bool same = !inject && b->last_jobs.size() == count && b->main.exec_stream == b->ctx->stream &&
+  const bool same = !inject && b->last_jobs.size() == count && b->main.stream == b->ctx->stream &&
                     memcmp(b->last_jobs.data(), jobs, count * sizeof(bntt_job)) == 0;
-  if (!same) {
+  if (!same) {  // a new list is launched directly; a graph is captured if it comes again
     b->last_jobs.clear();
     if (int rc = build_schedule(b, b->main, jobs, count)) return rc;
-    if (int rc = upload_and_capture(b, b->main, b->ctx->stream)) return rc;
+    if (int rc = upload(b, b->main, b->ctx->stream, false, false, b->upload_stream)) return rc;
     if (!inject) b->last_jobs.assign(jobs, jobs + count);
+  } else if (int rc = capture(b, b->main)) {
+    return rc;
   }
   b->inject_polls = 0;  // an injected fault lasts one run
   return launch_schedule(b, b->main, b->ctx->stream);
@@ -320,13 +411,15 @@ int bntt_batch_run_inverse_dev(bntt_batch* b, const bntt_job* jobs, size_t count
                "and the default arithmetic");
   for (bntt_plan* p : b->plans)
     if (int rc = plan_ensure_inverse(p)) return rc;
-  const bool same = b->inv_last_jobs.size() == count && b->inv.exec_stream == b->ctx->stream &&
+  const bool same = b->inv_last_jobs.size() == count && b->inv.stream == b->ctx->stream &&
                     memcmp(b->inv_last_jobs.data(), jobs, count * sizeof(bntt_job)) == 0;
   if (!same) {
     b->inv_last_jobs.clear();
     if (int rc = build_schedule(b, b->inv, jobs, count, true)) return rc;
-    if (int rc = upload_and_capture(b, b->inv, b->ctx->stream, true)) return rc;
+    if (int rc = upload(b, b->inv, b->ctx->stream, true, false, b->upload_stream)) return rc;
     b->inv_last_jobs.assign(jobs, jobs + count);
+  } else if (int rc = capture(b, b->inv)) {
+    return rc;
   }
   return launch_schedule(b, b->inv, b->ctx->stream);
 }
@@ -335,6 +428,8 @@ int bntt_batch_status(bntt_batch* b) {
   BNTT_REQUIRE(b, "NULL batch");
   if (int rc = ctx_use_device(b->ctx)) return rc;
   BNTT_CK(cudaStreamSynchronize(b->ctx->stream));
+  destroy_retired(b->main);
+  destroy_retired(b->inv);
   if (int rc = schedule_status(b->main)) return rc;
   if (int rc = schedule_status(b->inv)) return rc;
   for (Schedule& s : b->groups)
@@ -436,7 +531,8 @@ int bntt_batch_run_host_async(bntt_batch* b, const bntt_job* jobs, size_t count)
     for (size_t g = 0; g < ng; ++g) {
       const size_t f = b->group_first[g], e = b->group_first[g + 1];
       if (int rc = build_schedule(b, b->groups[g], dj.data() + f, e - f)) return rc;
-      if (int rc = upload_and_capture(b, b->groups[g], s_run, false, true)) return rc;
+      if (int rc = upload(b, b->groups[g], s_run, false, true)) return rc;
+      if (int rc = capture(b, b->groups[g])) return rc;
     }
     if (b->group_err_cap < ng) {
       if (b->group_err) cudaFreeHost(b->group_err);
@@ -501,6 +597,7 @@ int bntt_batch_sync(bntt_batch* b) {
   BNTT_CK(cudaStreamSynchronize(c->copy_stream[0]));
   BNTT_CK(cudaStreamSynchronize(c->stream));
   BNTT_CK(cudaStreamSynchronize(c->copy_stream[1]));
+  for (Schedule& s : b->groups) destroy_retired(s);
   if (!b->host_inflight && !b->host_err_pending) return BNTT_OK;
   b->host_inflight = false;
   return host_groups_status(b);

@@ -19,18 +19,29 @@ struct Schedule {
   std::vector<WorkItem> items;
   std::vector<uint32_t> pass_tiles;
   size_t nslots = 0;
-  void* d_jobs = nullptr;
-  size_t d_jobs_cap = 0;
-  void* d_order = nullptr;
-  size_t d_order_cap = 0;
-  void* d_items = nullptr;
-  size_t d_items_cap = 0;
-  void* d_ctl = nullptr;
+  // device copies of djobs, order, items and pass_tiles in one buffer, two
+  // buffers used in turn: a new job list is copied into the one the running
+  // launches do not read, so the copy overlaps them
+  void* d_sched[2] = {nullptr, nullptr};
+  size_t d_sched_cap[2] = {0, 0};
+  cudaEvent_t set_free[2] = {nullptr, nullptr};  // after the last launch reading d_sched[i]
+  bool set_used[2] = {false, false};
+  int cur = 1;                        // buffer of the current job list
+  cudaEvent_t set_ready = nullptr;    // the current list's copy has landed
+  void* d_ctl = nullptr;              // control words (queue head, error word, pass counters)
   size_t d_ctl_cap = 0;
-  void* d_pass_tiles = nullptr;
-  size_t d_pass_tiles_cap = 0;
-  cudaGraphExec_t exec = nullptr;
-  cudaStream_t exec_stream = nullptr;  // stream the graph was captured on
+  cudaGraphExec_t exec = nullptr;     // captured when the same job list runs again
+  std::vector<cudaGraphExec_t> retired;  // graphs of earlier job lists, destroyed once idle
+  // pinned staging of the uploads, two buffers used in turn: an upload waits
+  // only for the copy that read the same buffer two uploads before
+  void* stage[2] = {nullptr, nullptr};
+  size_t stage_cap[2] = {0, 0};
+  cudaEvent_t stage_done[2] = {nullptr, nullptr};
+  int stage_next = 0;
+  cudaStream_t stream = nullptr;      // stream the schedule was uploaded for
+  bool inverse = false;               // k_batch_inv instead of k_batch
+  bool sticky_err = false;            // launches leave the error word alone
+  BatchArgs args{};
   int grid = 0;
   size_t smem = 0;
 };
@@ -66,6 +77,7 @@ struct bntt_batch {
   // inverse runs (bntt_batch_run_inverse_dev)
   std::vector<bntt_job> inv_last_jobs;
   bntt::Schedule inv;
+  cudaStream_t upload_stream = nullptr;  // schedule copies of device-pointer runs
 };
 
 

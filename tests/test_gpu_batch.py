@@ -426,3 +426,32 @@ def test_run_host_async_reports_timeout_at_sync(ctx):
     s.engine.sync()
     assert np.array_equal(y, s.expected())
     s.close()
+
+
+def test_alternating_job_lists_without_sync(ctx):
+    """Two job lists (different sizes and outputs) queued in turn, with no
+    synchronisation in between: each new list is copied into the schedule
+    buffer the running launch does not read and launched directly; a list
+    seen again is replayed from its graph.  Both outputs equal the oracle."""
+    b = W.uneven_batch(seed=15, n_small=3000, large=((16, 2), (20, 1)))
+    s = Setup(ctx, b)
+    ya = DevBuf(ctx, b.total * 16)
+    yb = DevBuf(ctx, b.total * 16)
+    ids = [s.plan_ids[int(n)] for n in b.logns]
+    xs = [s.dx.addr + 16 * int(o) for o in b.offsets]
+    ja = bn.Batch.jobs(xs, [ya.addr + 16 * int(o) for o in b.offsets], ids)
+    half = b.count // 2
+    jb = bn.Batch.jobs(xs[half:][::-1], [yb.addr + 16 * int(o) for o in b.offsets[half:]][::-1], ids[half:][::-1])
+    for _ in range(3):
+        s.engine.run_dev(ja)
+        s.engine.run_dev(jb)
+    s.engine.run_dev(ja)
+    s.engine.run_dev(ja)             # the same list again: graph replay
+    assert s.engine.status() == bn.OK
+    want = s.expected()
+    assert np.array_equal(ya.to_array(b.total), want)
+    o = int(b.offsets[half])
+    assert np.array_equal(yb.to_array(b.total)[o:], want[o:])
+    ya.free()
+    yb.free()
+    s.close()
