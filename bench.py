@@ -59,7 +59,7 @@ def parse():
                     help="fraction of the uneven batch (profiling captures of a smaller case)")
     ap.add_argument("--headline-only", action="store_true",
                     help="only the persistent-kernel step (for profiler launch lists)")
-    ap.add_argument("--only", choices=["uniform", "inverse", "blas", "serving"], default=None,
+    ap.add_argument("--only", choices=["uniform", "inverse", "inverse_batch", "blas", "serving"], default=None,
                     help="run one secondary benchmark alone (profiling captures)")
     ap.add_argument("--logn", type=int, default=10, help="size for --only uniform")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -254,6 +254,8 @@ def run_only(args, dist: Dist):
                             inverse=args.only == "inverse")
     elif args.only == "serving":
         res = serving_bench(args, ctx)
+    elif args.only == "inverse_batch":
+        res = inverse_batch_only(args, ctx, stream)
     else:
         res = blas_bench(args, ctx, stream, measured_peaks())
     return {"only": args.only, "result": res}, ctx
@@ -631,6 +633,39 @@ def uniform_bench(args, ctx, stream, imad_peak, sizes=(4, 5, 6, 7, 8, 9, 10, 16,
                        "l2": "flushed before each timed launch" if small else "inputs larger than L2"}
         plan.close()
         del x, y
+    return res
+
+
+def inverse_batch_only(args, ctx, stream) -> dict:
+    """The inverse batch alone on the uneven batch (scaled by --scale), for
+    profiling k_batch_inv."""
+    import torch
+
+    import benchntt_b200 as bn
+    from benchntt_b200 import workloads as W
+    L = bn.lib()
+    batch = W.uneven_batch()
+    if args.scale < 1.0:
+        large = tuple((l, max(1, int(c * args.scale))) for l, c in ((16, 64), (20, 4)))
+        batch = W.uneven_batch(n_small=max(1, int(100_000 * args.scale)), large=large)
+    mod = bn.modulus(Q_NTT, MU_NTT)
+    plans = {n: bn.Plan(ctx, n, Q_NTT, MU_NTT, bn.fill_uniform(W.SEED_TWIDDLE_BASE + n, 1 << n, Q_NTT))
+             for n in batch.sizes}
+    pid = {n: i for i, n in enumerate(batch.sizes)}
+    x = torch.empty((batch.total, 2), dtype=torch.int64, device=ctx.device)
+    y = torch.empty_like(x)
+    bn.check(L.bntt_fill_uniform_dev(ctx.handle, x.data_ptr(), batch.total, W.SEED_INPUT, 0,
+                                     ctypes.byref(mod), 0))
+    engine = bn.Batch(ctx, [plans[n] for n in batch.sizes])
+    offs = batch.offsets * 16
+    jobs = bn.Batch.jobs([x.data_ptr() + int(o) for o in offs], [y.data_ptr() + int(o) for o in offs],
+                         [pid[int(n)] for n in batch.logns])
+    res = inverse_batch_bench(args, ctx, stream, engine, jobs, batch, 1.0)
+    res.pop("vs_forward")
+    res["transforms"] = batch.count
+    engine.close()
+    for p in plans.values():
+        p.close()
     return res
 
 

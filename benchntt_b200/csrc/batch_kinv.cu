@@ -51,13 +51,9 @@ __device__ __noinline__ void run_item_engine_inv(const WorkItem& it, const Batch
   // the store that finishes a transform applies N^-1
   const bool finishes = it.kind == ITEM_SMALL || it.pass == 0;
   Epilogue ep;
-  if (finishes) {
-    const uint4 f = __ldg(it.kind == ITEM_SMALL ? sr.tw : ba.jobs[it.a].tw);  // N^-1
-    ep.scale = U128{{f.x, f.y, f.z, f.w}};
-    ep.has_scale = 1;
-  }
-  E::template run<LD_CG, true, EPI_SCALE>(m, map, kBatchThreads, sr, sub, lane, smem, mp, layout,
-                                     finishes ? &ep : nullptr);
+  ep.scale_at = it.kind == ITEM_SMALL ? sr.tw : ba.jobs[it.a].tw;  // N^-1
+  E::template run<LD_CG, true, EPI_SCALE_AT>(m, map, kBatchThreads, sr, sub, lane, smem, mp, layout,
+                                        finishes ? &ep : nullptr);
   item_publish(it, ba);
 }
 

@@ -64,11 +64,13 @@ struct MulB {
 };
 
 // What the last store of an engine kernel applies (ntt_engine.cuh): an
-// optional scalar multiply (the inverse transform's N^-1), then an optional
-// pointwise product (MulB).
+// optional scalar multiply (the inverse transform's N^-1, held here or read
+// at the store from device memory), then an optional pointwise product
+// (MulB).
 struct Epilogue {
   U128 scale{};
   int has_scale = 0;
+  const uint4* scale_at = nullptr;  // EPI_SCALE_AT: the scalar, limb order
   MulB mul;
 };
 

@@ -17,7 +17,7 @@
 
 namespace bntt {
 
-enum : int { EPI_SCALE = 1, EPI_MUL = 2 };
+enum : int { EPI_SCALE = 1, EPI_MUL = 2, EPI_SCALE_AT = 4 };
 
 template <int LOGR, class Arith>
 struct NttEngine {
@@ -76,7 +76,8 @@ struct NttEngine {
   // INV runs the inverse of the same r stages: the stages in reverse order,
   // each an inverse (Gentleman-Sande) butterfly with the table holding the
   // inverse twiddles.  EPI applies *ep (when not null) on the last store:
-  // bit EPI_SCALE its scalar multiply, bit EPI_MUL its pointwise product.
+  // bit EPI_SCALE its scalar multiply, EPI_SCALE_AT the multiply by the
+  // scalar at ep->scale_at, bit EPI_MUL its pointwise product.
   template <int r, int LDP, bool INV = false, int EPI = 0>
   __device__ __forceinline__ static void pass(U128 (&v)[R], const SubRef& sr, int s0, int lo,
                                               int lane, int tpt, bool first, bool last,
@@ -149,6 +150,10 @@ struct NttEngine {
               if (ep) {
                 if constexpr ((EPI & EPI_SCALE) != 0) {
                   if (ep->has_scale) v[i * G + j] = Arith::mul(v[i * G + j], ep->scale, mp);
+                }
+                if constexpr ((EPI & EPI_SCALE_AT) != 0) {  // loaded here: nothing held across the pass
+                  const uint4 f = __ldg(ep->scale_at);
+                  v[i * G + j] = Arith::mul(v[i * G + j], U128{{f.x, f.y, f.z, f.w}}, mp);
                 }
                 if ((EPI & EPI_MUL) != 0 && ep->mul.b) {
                   const uint4 bv = __ldg(ep->mul.b + ((uint64_t)(yp - ep->mul.ybase) & ep->mul.bmask));
