@@ -36,7 +36,8 @@ __device__ __noinline__ void run_item_tiny_inv(const WorkItem& it, const BatchAr
   const uint4 f = __ldg(sr.tw);  // N^-1
   const U128 ninv = U128{{f.x, f.y, f.z, f.w}};
 #pragma unroll
-  for (int i = 0; i < N; ++i) sr.y[i] = to_mem(ArithFast::mul(v[i], ninv, mp), layout);
+  for (int i = 0; i < N; ++i)  // the second half carries N^-1 through table entry 1
+    sr.y[i] = to_mem(i < N / 2 ? ArithFast::mul(v[i], ninv, mp) : v[i], layout);
 }
 
 __device__ __noinline__ void run_item_engine_inv(const WorkItem& it, const BatchArgs& ba, uint4* smem,

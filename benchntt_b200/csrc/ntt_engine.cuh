@@ -148,12 +148,17 @@ struct NttEngine {
             uint4* yp = gq + (size_t)(j * gstep);
             if constexpr (EPI != 0) {
               if (ep) {
+                // the inverse's N^-1: the upper half of the group holds y
+                // outputs of the last stage, whose table entry carries it
+                const bool scaled = !INV || j < G / 2;
                 if constexpr ((EPI & EPI_SCALE) != 0) {
-                  if (ep->has_scale) v[i * G + j] = Arith::mul(v[i * G + j], ep->scale, mp);
+                  if (ep->has_scale && scaled) v[i * G + j] = Arith::mul(v[i * G + j], ep->scale, mp);
                 }
                 if constexpr ((EPI & EPI_SCALE_AT) != 0) {  // loaded here: nothing held across the pass
-                  const uint4 f = __ldg(ep->scale_at);
-                  v[i * G + j] = Arith::mul(v[i * G + j], U128{{f.x, f.y, f.z, f.w}}, mp);
+                  if (scaled) {
+                    const uint4 f = __ldg(ep->scale_at);
+                    v[i * G + j] = Arith::mul(v[i * G + j], U128{{f.x, f.y, f.z, f.w}}, mp);
+                  }
                 }
                 if ((EPI & EPI_MUL) != 0 && ep->mul.b) {
                   const uint4 bv = __ldg(ep->mul.b + ((uint64_t)(yp - ep->mul.ybase) & ep->mul.bmask));

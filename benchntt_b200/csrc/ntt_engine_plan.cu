@@ -76,7 +76,8 @@ __global__ void __launch_bounds__(256)
       gs_butterfly<ArithFast>(v[i], v[i + half], U128{{tv.x, tv.y, tv.z, tv.w}}, mp);
     }
   }
-  for (int i = 0; i < N; ++i) x[t * N + i] = to_mem(ArithFast::mul(v[i], scale, mp), layout);
+  // the second half already carries N^-1 through table entry 1
+  for (int i = 0; i < N; ++i) x[t * N + i] = to_mem(i < N / 2 ? ArithFast::mul(v[i], scale, mp) : v[i], layout);
 }
 
 template <bool INV>
@@ -134,8 +135,16 @@ int engine_passes(bntt_plan* p, void* out, const void* in, size_t batch, const v
 // Inverse table (T[k]^-1, limb order) and N^-1, built once per plan: the
 // forward table comes back from the device and is inverted on the host with
 // one modular exponentiation and three multiplies per entry (batch
-// inversion).  Entry 0, which no network stage reads, holds N^-1: the
-// inverse batch kernel takes each job's scale from its own table.
+// inversion).  Entry 0, which no network stage reads, holds N^-1 (the
+// inverse batch kernel takes each job's scale from its own table), and
+// entry 1 holds T[1]^-1 * N^-1: every inverse kernel then scales only the
+// first half of its outputs (the x outputs of the last stage).
+static u128 entry_of(const std::vector<uint32_t>& t, size_t k) {
+  u128 v = 0;
+  for (int l = 3; l >= 0; --l) v = (v << 32) | t[4 * k + l];
+  return v;
+}
+
 int ensure_inverse(bntt_plan* p) {
   if (p->tw_inv) return BNTT_OK;
   const u128 q = to_u128(p->mod.q), mu = to_u128(p->mod.mu);
@@ -171,6 +180,10 @@ int ensure_inverse(bntt_plan* p) {
   const u128 ninv = host_powmod((u128)n % q, q - 2, q, mu);
   BNTT_REQUIRE(host_mulmod(ninv, (u128)n % q, q, mu) == 1, "N has no inverse mod q");
   for (int l = 0; l < 4; ++l) ti[l] = (uint32_t)(ninv >> (32 * l));
+  // entry 1 (the last inverse stage, which ends in y = (x - y) * T[1]^-1)
+  // carries N^-1 too, so the final scaling multiplies the x half only
+  const u128 t1 = host_mulmod(entry_of(ti, 1), ninv, q, mu);
+  for (int l = 0; l < 4; ++l) ti[4 + l] = (uint32_t)(t1 >> (32 * l));
   void* d = nullptr;
   if (int rc = ctx_alloc(p->ctx, &d, n * 16)) return rc;
   cudaError_t e = cudaMemcpyAsync(d, ti.data(), n * 16, cudaMemcpyHostToDevice, p->ctx->stream);
