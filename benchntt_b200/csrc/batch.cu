@@ -44,12 +44,12 @@ using namespace bntt;
 
 namespace bntt {
 
-int grow(bntt_ctx* c, void** p, size_t* cap, size_t bytes) {
+int grow(bntt_ctx* c, void** p, size_t* cap, size_t bytes, bool headroom) {
   if (*cap >= bytes && *p) return BNTT_OK;
-  if (*p) ctx_free(c, *p);
+  if (*p) ctx_free(c, *p);  // waits for the device: rare with headroom
   *p = nullptr;
   *cap = 0;
-  const size_t want = std::max<size_t>(bytes, 256);
+  const size_t want = std::max<size_t>(headroom ? bytes + bytes / 4 : bytes, 256);
   if (int rc = ctx_alloc(c, p, want)) return rc;
   *cap = want;
   return BNTT_OK;
@@ -200,8 +200,8 @@ static int upload(bntt_batch* b, Schedule& sc, cudaStream_t stream, bool inverse
   }
   const int set = sc.cur ^ 1;
   cudaStream_t cs = copy_stream ? copy_stream : stream;
-  if (int rc = grow(c, &sc.d_sched[set], &sc.d_sched_cap[set], total)) return rc;
-  if (int rc = grow(c, &sc.d_ctl, &sc.d_ctl_cap, cb)) return rc;
+  if (int rc = grow(c, &sc.d_sched[set], &sc.d_sched_cap[set], total, true)) return rc;
+  if (int rc = grow(c, &sc.d_ctl, &sc.d_ctl_cap, cb, true)) return rc;
   if (sc.set_used[set] && cs != stream) BNTT_CK(cudaStreamWaitEvent(cs, sc.set_free[set], 0));
   const int si = sc.stage_next;
   sc.stage_next ^= 1;

@@ -82,7 +82,8 @@ struct bntt_batch {
 
 
 namespace bntt {
-int grow(bntt_ctx* c, void** p, size_t* cap, size_t bytes);
+// device buffer of at least `bytes` (headroom: a quarter more when it grows)
+int grow(bntt_ctx* c, void** p, size_t* cap, size_t bytes, bool headroom = false);
 void free_schedule(bntt_ctx* c, Schedule& s);
 const void* batch_kernel(bool fast);
 const void* batch_kernel_inverse();
