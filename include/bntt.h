@@ -212,8 +212,8 @@ int bntt_batch_destroy(bntt_batch *batch);
 /* Device pointers, asynchronous.  The schedule (work items, their order and
  * the per-size kernel shapes) is rebuilt only when the job list changes: a
  * new list is built on the host and copied while earlier launches run, then
- * launched; a list run again is replayed from a CUDA graph.  Nothing here
- * waits for the device. */
+ * launched; a list run again is replayed from a CUDA graph.  Only a list
+ * larger than any before (its buffers grow) waits for the device. */
 int bntt_batch_run_dev(bntt_batch *batch, const bntt_job *jobs, size_t count);
 /* Host pointers: inputs copied in, batch run, outputs copied back. */
 int bntt_batch_run_host(bntt_batch *batch, const bntt_job *jobs, size_t count);
