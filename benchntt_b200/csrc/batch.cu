@@ -81,15 +81,26 @@ void free_schedule(bntt_ctx* c, Schedule& s) {
 
 const void* batch_kernel(bool fast) { return fast ? batch_kernel_fast_minb(g_batch_minb) : batch_kernel_ref(); }
 
+constexpr int kMaxLog2n = 24;  // plans hold 2^1..2^24 points
+
+// engine_split for every size a batch job can have, computed once.
+static const std::vector<int>& split_of(int n) {
+  static const std::vector<std::vector<int>> table = [] {
+    std::vector<std::vector<int>> t(kMaxLog2n + 1);
+    for (int m = 11; m <= kMaxLog2n; ++m) t[m] = engine_split(m);
+    return t;
+  }();
+  return table[n];
+}
+
 int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count,
                    bool inverse) {
   sc.djobs.resize(count);
-  sc.order.clear();
   sc.items.clear();
   sc.pass_tiles.clear();
   sc.nslots = 0;
-  std::vector<uint32_t> by_size[11];
-  std::vector<uint32_t> large;
+  // one pass over the jobs: descriptors, the count of small jobs per size
+  uint32_t per_size[11] = {};
   for (size_t i = 0; i < count; ++i) {
     const bntt_job& jb = jobs[i];
     BNTT_REQUIRE(jb.plan < b->plans.size(), "job %zu: plan index %u out of range", i, jb.plan);
@@ -101,21 +112,34 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
     d.y = static_cast<uint4*>(jb.y);
     d.tw = static_cast<const uint4*>(inverse ? p->tw_inv : p->tw);
     d.log2n = p->log2n;
-    d.slot = 0;
     if (p->log2n <= 10) {
-      by_size[p->log2n].push_back((uint32_t)i);
+      d.slot = 0;
+      ++per_size[p->log2n];
     } else {
       d.slot = (uint32_t)sc.nslots++;
-      large.push_back((uint32_t)i);
     }
   }
-  std::vector<WorkItem> later[kMaxPasses];
+  // small jobs in size order, largest size first (a counting sort)
+  uint32_t first[11] = {}, fill[11];
+  uint32_t small = 0;
+  for (int n = 10; n >= 1; --n) {
+    first[n] = small;
+    small += per_size[n];
+  }
+  std::copy(first, first + 11, fill);
+  sc.order.resize(small);
+  for (size_t i = 0; i < count; ++i) {
+    const uint32_t n = sc.djobs[i].log2n;
+    if (n <= 10) sc.order[fill[n]++] = (uint32_t)i;
+  }
+  for (auto& l : sc.later) l.clear();
   sc.pass_tiles.assign(sc.nslots * kMaxPasses, 0);
-  for (uint32_t ji : large) {
+  for (size_t ji = 0; ji < count; ++ji) {
     const DevJob& d = sc.djobs[ji];
+    if (d.log2n <= 10) continue;
     const int n = (int)d.log2n;
-    const std::vector<int> passes = engine_split(n);
-    BNTT_REQUIRE(passes.size() <= (size_t)kMaxPasses, "log2n %d needs too many passes", n);
+    const std::vector<int>& passes = split_of(n);
+    BNTT_REQUIRE(!passes.empty() && passes.size() <= (size_t)kMaxPasses, "log2n %d needs too many passes", n);
     int s0 = 0;
     for (size_t p = 0; p < passes.size(); ++p) {
       const int m = passes[p];
@@ -129,41 +153,39 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
       // position in the run order: forward pass p runs p-th, the inverse runs
       // the passes last to first
       const size_t run = inverse ? passes.size() - 1 - p : p;
+      std::vector<WorkItem>& q = sc.later[run];
+      WorkItem w{};
+      w.shape = (uint16_t)shape;
+      w.kind = ITEM_PASS;
+      w.a = (uint32_t)ji;
+      w.pass = (uint16_t)p;
+      w.wait = (uint16_t)((run > 0 ? 1 : 0) | (run == 0 ? 2 : 0) | (s0 << 8));
       for (uint32_t t = 0; t < tiles; ++t) {
-        WorkItem w{};
-        w.shape = (uint16_t)shape;
-        w.kind = ITEM_PASS;
-        w.a = ji;
         w.b = t * tpc;
-        w.pass = (uint16_t)p;
-        w.wait = (uint16_t)((run > 0 ? 1 : 0) | (run == 0 ? 2 : 0) | (s0 << 8));
-        later[run].push_back(w);
+        q.push_back(w);
       }
       s0 += m;
     }
   }
   // queue: passes that run first, small tiles (largest size first), the
   // other passes in run order
-  for (const WorkItem& w : later[0]) sc.items.push_back(w);
+  sc.items.insert(sc.items.end(), sc.later[0].begin(), sc.later[0].end());
   for (int n = 10; n >= 1; --n) {
-    const std::vector<uint32_t>& v = by_size[n];
-    if (v.empty()) continue;
+    const uint32_t cnt = per_size[n];
+    if (cnt == 0) continue;
     const int shape = b->shapes.small[n];
     BNTT_REQUIRE(shape >= 0, "no batch shape for size 2^%d", n);
     const uint32_t tpc = (uint32_t)kShapes[shape].tpc;
-    const uint32_t base = (uint32_t)sc.order.size();
-    sc.order.insert(sc.order.end(), v.begin(), v.end());
-    for (uint32_t s = 0; s < v.size(); s += tpc) {
-      WorkItem w{};
-      w.shape = (uint16_t)shape;
-      w.kind = ITEM_SMALL;
-      w.a = base + s;
-      w.b = std::min<uint32_t>(tpc, (uint32_t)v.size() - s);
+    WorkItem w{};
+    w.shape = (uint16_t)shape;
+    w.kind = ITEM_SMALL;
+    for (uint32_t s = 0; s < cnt; s += tpc) {
+      w.a = first[n] + s;
+      w.b = std::min<uint32_t>(tpc, cnt - s);
       sc.items.push_back(w);
     }
   }
-  for (int p = 1; p < kMaxPasses; ++p)
-    for (const WorkItem& w : later[p]) sc.items.push_back(w);
+  for (int p = 1; p < kMaxPasses; ++p) sc.items.insert(sc.items.end(), sc.later[p].begin(), sc.later[p].end());
   return BNTT_OK;
 }
 

@@ -18,6 +18,7 @@ struct Schedule {
   std::vector<uint32_t> order;
   std::vector<WorkItem> items;
   std::vector<uint32_t> pass_tiles;
+  std::vector<WorkItem> later[kMaxPasses];  // build scratch: pass items by run position
   size_t nslots = 0;
   // device copies of djobs, order, items and pass_tiles in one buffer, two
   // buffers used in turn: a new job list is copied into the one the running
