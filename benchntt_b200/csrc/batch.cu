@@ -5,6 +5,8 @@
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "batch_host.h"
 
@@ -28,6 +30,33 @@ size_t shape_smem(int s) {
   if (npass <= 1) return 0;
   if (b.m <= 2) return (size_t)b.tpc * ((size_t)1 << b.m) * 16;  // one-thread tiles
   return NttEngine<3, ArithFast>::smem_slots(b.m, b.map, kBatchThreads) * 16;
+}
+
+// Resident CTAs per SM of a batch kernel (forward or inverse) at the largest
+// tile's shared memory, per device.  Every tile fits the default 48 KB of
+// dynamic shared memory, so no launch raises the kernel's limit: a limit set
+// for one job list (and lowered for the next) would fail launches of others
+// that share the kernel, such as the serving loop's.
+int batch_kernel_bps(const void* fn, int* bps) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> cache;
+  int dev = 0;
+  BNTT_CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  auto it = cache.find({fn, dev});
+  if (it != cache.end()) {
+    *bps = it->second;
+    return BNTT_OK;
+  }
+  size_t smem = 0;
+  for (int k = 0; k < kNumShapes; ++k) smem = std::max(smem, shape_smem(k));
+  BNTT_REQUIRE(smem <= 48 * 1024, "batch tile needs %zu bytes of shared memory", smem);
+  int b = 0;
+  BNTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kBatchThreads, smem));
+  if (b < 1) return set_error(BNTT_ECUDA, "batch kernel does not fit on an SM (smem %zu)", smem);
+  cache[{fn, dev}] = b;
+  *bps = b;
+  return BNTT_OK;
 }
 
 // First shape for (m, map) with the preferred radix (0 = any).
@@ -267,10 +296,8 @@ static int upload(bntt_batch* b, Schedule& sc, cudaStream_t stream, bool inverse
   for (const WorkItem& w : sc.items) used[w.shape] = true;
   for (int s = 0; s < kNumShapes; ++s)
     if (used[s]) smem = std::max(smem, shape_smem(s));
-  BNTT_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1)));
   int bps = 0;
-  BNTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, kBatchThreads, smem));
-  if (bps < 1) return set_error(BNTT_ECUDA, "batch kernel does not fit on an SM (smem %zu)", smem);
+  if (int rc = batch_kernel_bps(fn, &bps)) return rc;
   sc.grid = (int)std::min<size_t>((size_t)bps * c->sms, sc.items.size());
   sc.smem = smem;
   BatchArgs& ba = sc.args;
@@ -776,10 +803,8 @@ extern "C" int bntt_batch_run_dev_noalloc(bntt_batch* b, const bntt_job* jobs, s
   for (const WorkItem& w : sc.items) used[w.shape] = true;
   for (int k = 0; k < kNumShapes; ++k)
     if (used[k]) smem = std::max(smem, shape_smem(k));
-  BNTT_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1)));
   int bps = 0;
-  BNTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, kBatchThreads, smem));
-  if (bps < 1) return set_error(BNTT_ECUDA, "batch kernel does not fit on an SM (smem %zu)", smem);
+  if (int rc = batch_kernel_bps(fn, &bps)) return rc;
   const unsigned grid = (unsigned)std::min<size_t>((size_t)bps * c->sms, sc.items.size());
   BatchArgs ba;
   ba.items = reinterpret_cast<const WorkItem*>(s + o_it);

@@ -88,6 +88,8 @@ int grow(bntt_ctx* c, void** p, size_t* cap, size_t bytes, bool headroom = false
 void free_schedule(bntt_ctx* c, Schedule& s);
 const void* batch_kernel(bool fast);
 const void* batch_kernel_inverse();
+// resident CTAs per SM of a batch kernel (cached per device)
+int batch_kernel_bps(const void* fn, int* bps);
 size_t shape_smem(int s);
 // inverse = true: the jobs' inverse transforms (plans' inverse tables, the
 // passes of a large job queued last to first)

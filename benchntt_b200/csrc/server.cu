@@ -140,6 +140,7 @@ struct bntt_server {
   std::atomic<bool> stop{false};
   std::atomic<uint64_t> submitted{0}, completed{0}, launches{0}, admission_waits{0};
   int worker_error = BNTT_OK;
+  int batch_bps = 0;  // resident batch-kernel CTAs per SM
 
   double now() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -192,10 +193,9 @@ static int launch_slot(bntt_server* s, Slot& slot) {
     const void* fn = batch_kernel(s->engine->fast);
     size_t smem = 0;
     for (const WorkItem& w : sc.items) smem = std::max(smem, shape_smem(w.shape));
-    BNTT_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1)));
-    int bps = 0;
-    BNTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, kBatchThreads, smem));
-    const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((size_t)bps * c->sms, sc.items.size()));
+    // occupancy queried once at creation
+    const unsigned grid =
+        (unsigned)std::max<size_t>(1, std::min<size_t>((size_t)s->batch_bps * c->sms, sc.items.size()));
     BatchArgs ba;
     ba.items = reinterpret_cast<const WorkItem*>(d + o_it);
     ba.nitems = (uint32_t)sc.items.size();
@@ -329,6 +329,12 @@ int bntt_server_create(bntt_ctx* c, bntt_server** out, bntt_plan* const* plans, 
     return rc;
   }
   s->arena.init(static_cast<char*>(s->arena_mem), s->cfg.hbm_budget);
+  if ((rc = batch_kernel_bps(batch_kernel(s->engine->fast), &s->batch_bps))) {
+    ctx_free(c, s->arena_mem);
+    bntt_batch_destroy(s->engine);
+    delete s;
+    return rc;
+  }
   bool fast = false;
   s->blas_mp = make_params(*blas_modulus, &fast);
   s->blas_fast = arith_fast(c, fast);

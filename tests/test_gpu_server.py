@@ -171,3 +171,30 @@ def test_launch_output_cap():
     assert st["launches"] >= 4
     assert st["completed"] == 7
     fx.close()
+
+
+def test_other_batches_do_not_break_server_launches():
+    """A batch of only the tiniest transforms (one-thread tiles, the least
+    shared memory) runs between server launches: the server's later launches
+    of 2^10-point tiles still run and are correct (no shared-memory limit of
+    the common kernel is set per job list)."""
+    fx = Fixture(slots=1)
+    tiny_t = C.uniform_pairs(61, 2, C.Q_NTT)
+    tiny_plan = bn.Plan(fx.ctx, 1, C.Q_NTT, C.MU_NTT, tiny_t)
+    tiny_engine = bn.Batch(fx.ctx, [tiny_plan])
+    xt = C.uniform_pairs(62, 2 * 64, C.Q_NTT)
+    dxt, dyt = fx.dev(xt), fx.dev(np.zeros_like(xt))
+    jobs = bn.Batch.jobs([dxt.addr + 32 * i for i in range(64)], [dyt.addr + 32 * i for i in range(64)], [0] * 64)
+    n = 10
+    pi = NTT_SIZES.index(n)
+    x = C.uniform_pairs(63, 1 << n, C.Q_NTT)
+    r = bn.RequestC(bn.REQ_NTT, pi, 0, fx.dev(x).addr, None, bn.U128.of(0), 0, 0.0)
+    run_mix(fx, [r])
+    tiny_engine.run_dev(jobs)
+    assert tiny_engine.status() == bn.OK
+    out = run_mix(fx, [r])
+    assert np.array_equal(out[0], C.oracle_ntt(x, fx.tables[n], n))
+    assert np.array_equal(dyt.to_array(128), C.oracle_ntt(xt, tiny_t, 1))
+    tiny_engine.close()
+    tiny_plan.close()
+    fx.close()
