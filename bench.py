@@ -6,9 +6,12 @@ Headline workload (one "step"): the uneven batch -- 100,000 forward 128-bit
 NTTs with N log-uniform over 2^4..2^10 plus 64 at 2^16 and 4 at 2^20 (modulus
 2^124 - 719 of the reference NTT drivers), run by one graph launch of the
 persistent work-queue kernel.  `value` is transforms per second with inputs
-resident in HBM; `e2e` is the same metric through bntt_batch_run_host from
-pinned host buffers (copies in and out inside the timed region).  The same
-line carries the per-call GPU path on the same jobs, the BLAS ops at 2^24
+resident in HBM; `e2e` is the same metric from pinned host buffers, every
+step one bntt_batch_run_host_async call (all inputs copied in, all outputs
+copied out) queued back to back with one bntt_batch_sync at the end, and
+beside it one synchronous bntt_batch_run_host per step.  The same line
+carries a new job list every step, the inverse batch, the per-call GPU path
+on the same jobs, the BLAS ops at 2^24
 elements in GB/s, uniform batches of 65,536 transforms per size, the roofline
 of the persistent kernel against the measured IMAD pipe peak, the reference's
 CPU throughput on the same workload (timed on this host's cores), and the SM
@@ -418,8 +421,8 @@ def measured_peaks() -> dict:
 
 
 def e2e_uneven(args, dist, ctx, engine, batch, pid) -> dict:
-    """bntt_batch_run_host from pinned host buffers: every step copies all
-    inputs in and all outputs out."""
+    """The uneven batch from pinned host buffers: every step copies all
+    inputs in and all outputs out (queued steps, and one call at a time)."""
     import torch
 
     import benchntt_b200 as bn
