@@ -381,6 +381,8 @@ def run_ours(args, dist: Dist):
     result["new_job_list_each_step"] = fresh_lists(args, ctx, stream, engine, jobs, batch, value)
     # ---------------------------------------------------------- per-call path
     result["per_call"] = per_call(args, dist, ctx, stream, engine, jobs, batch, value)
+    # ------------------------------------- one transform of N = 1024 per call
+    result["single_ntt_1024"] = single_ntt(args, ctx, stream)
     # ----------------------------------------------------------------- BLAS
     result["blas"] = blas_bench(args, ctx, stream, peaks)
     # --------------------------------------------------------- uniform sizes
@@ -491,6 +493,52 @@ def pcie_both_ways(xh, yh) -> float:
     dt = (time.perf_counter() - t0) / 3
     del dx, dy
     return xh.numel() * 8 / dt / 1e9
+
+
+def single_ntt(args, ctx, stream, logn: int = 10) -> dict:
+    """One forward NTT of N = 1024 per call, the reference programs' unit of
+    work (src/ntt_scalar.c:582): the plain one-launch device path (calls back
+    to back on one stream, and one call with the host waiting for it), and the
+    host call that copies the input in and the output out (plan cached)."""
+    import torch
+
+    import benchntt_b200 as bn
+    from benchntt_b200 import workloads as W
+    L = bn.lib()
+    n = 1 << logn
+    plan = bn.Plan(ctx, logn, Q_NTT, MU_NTT, bn.fill_uniform(W.SEED_TWIDDLE_BASE + logn, n, Q_NTT))
+    x = torch.empty((n, 2), dtype=torch.int64, device=ctx.device)
+    y = torch.empty_like(x)
+    mod = bn.modulus(Q_NTT, MU_NTT)
+    bn.check(L.bntt_fill_uniform_dev(ctx.handle, x.data_ptr(), n, 5, 0, ctypes.byref(mod), 0))
+    for _ in range(20):
+        plan.forward(y, x, 1)
+    torch.cuda.synchronize()
+    reps = 200
+    e0, e1 = cuda_events()
+    e0.record(stream)
+    for _ in range(reps):
+        plan.forward(y, x, 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    back_to_back_us = e0.elapsed_time(e1) / reps * 1e3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        plan.forward(y, x, 1)
+        torch.cuda.synchronize()
+    sync_us = (time.perf_counter() - t0) / reps * 1e6
+    xh = bn.fill_uniform(5, n, Q_NTT)
+    yh = np.empty_like(xh)
+    for _ in range(10):
+        plan.forward(yh, xh)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        plan.forward(yh, xh)
+    host_us = (time.perf_counter() - t0) / reps * 1e6
+    plan.close()
+    return {"n": n, "device_us_per_call_back_to_back": back_to_back_us,
+            "device_us_per_call_waited": sync_us, "host_buffers_us_per_call": host_us,
+            "api": "bntt_ntt_forward_dev / bntt_ntt_forward_host, batch = 1"}
 
 
 def fresh_lists(args, ctx, stream, engine, jobs, batch, batched_value) -> dict:
@@ -950,6 +998,10 @@ def main():
             # the same CPU sample per size: the reference's throughput on the
             # uniform batches (all cores, one transform per core at a time)
             cores = res["cpu_baseline"]["cores"]
+            one = res.get("single_ntt_1024")
+            secs = res["cpu_baseline"].get("seconds_per_transform", {}).get("1024")
+            if one and secs:   # one core per transform, as the reference programs run
+                one["cpu_reference_us_per_transform"] = secs * 1e6
             for n, secs in res["cpu_baseline"].get("seconds_per_transform", {}).items():
                 row = res.get("uniform", {}).get(n)
                 if row and secs > 0:
