@@ -142,9 +142,9 @@ int plan_choose_kernels(bntt_plan* p) {
     // that fits (interleaved tiles need TPC adjacent columns, so TPC <= 2^l)
     const SubKernel* k = tuned_sub_kernel(m, map, fast ? 1 : 0, l);
     // untuned contiguous passes with the fast multiply: the 4-element shape
-    // capped at 4 resident CTAs per SM (2^3..2^8), else the shape capped at 3
-    // (2^9, 2^10) -- the autotuner's picks on B200; without a cap the
-    // compiler spends up to 214 registers and one CTA fills the SM
+    // capped at 4 resident CTAs per SM (2^3..2^10), else the shape capped at
+    // 3 -- measured on B200; without a cap the compiler spends up to 214
+    // registers and one CTA fills the SM
     for (int want_minb : {4, 3}) {
       for (const SubKernel& c : sub_kernels()) {
         if (k || map != MAP_CONTIG || !fast) break;
