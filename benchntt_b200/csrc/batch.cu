@@ -5,6 +5,7 @@
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <mutex>
 
@@ -19,17 +20,18 @@ const void* batch_kernel_ref();
 // autotuner may change it.  BNTT_BATCH_MINB overrides it at start-up.
 static std::atomic<int> g_batch_minb{[] {
   const char* e = getenv("BNTT_BATCH_MINB");
-  return (e && atoi(e) == 2) ? 2 : 3;
+  const int v = e ? atoi(e) : 4;
+  return v == 2 || v == 3 ? v : 4;
 }()};
 int batch_minb() { return g_batch_minb.load(std::memory_order_relaxed); }
-void set_batch_minb(int m) { g_batch_minb.store(m == 2 ? 2 : 3, std::memory_order_relaxed); }
+void set_batch_minb(int m) { g_batch_minb.store(m == 2 || m == 3 ? m : 4, std::memory_order_relaxed); }
 
 size_t shape_smem(int s) {
   const BatchShape& b = kShapes[s];
   const int npass = (b.m + b.logr - 1) / b.logr;
   if (npass <= 1) return 0;
   if (b.m <= 2) return (size_t)b.tpc * ((size_t)1 << b.m) * 16;  // one-thread tiles
-  return NttEngine<3, ArithFast>::smem_slots(b.m, b.map, kBatchThreads) * 16;
+  return NttEngine<kBatchLogR, ArithFast>::smem_slots(b.m, b.map, kBatchThreads) * 16;
 }
 
 // Resident CTAs per SM of a batch kernel (forward or inverse) at the largest
@@ -112,11 +114,44 @@ const void* batch_kernel(bool fast) { return fast ? batch_kernel_fast_minb(g_bat
 
 constexpr int kMaxLog2n = 24;  // plans hold 2^1..2^24 points
 
-// engine_split for every size a batch job can have, computed once.
+// HBM passes of a large batch job: the fewest passes, then the fewest
+// engine passes (a pass of m stages is ceil(m / 2) of them).  A strided pass
+// (all but the last) has 5..7 stages, so its tile of 2^(10 - m) adjacent
+// columns covers at least 128 bytes of each row, and needs that many columns
+// (2^(10 - m) <= 2^l); the last, contiguous pass has 3..10 stages.
+static std::vector<int> batch_split(int n) {
+  std::vector<int> best, cur;
+  int best_passes = 1 << 30, best_cost = 1 << 30;
+  std::function<void(int, int, int)> rec = [&](int s0, int cost, int depth) {
+    const int left = n - s0;
+    if (left >= 3 && left <= 10) {  // finish with a contiguous pass
+      cur.push_back(left);
+      const int passes = (int)cur.size(), c = cost + (left + 1) / 2;
+      if (passes < best_passes || (passes == best_passes && c < best_cost)) {
+        best_passes = passes;
+        best_cost = c;
+        best = cur;
+      }
+      cur.pop_back();
+    }
+    if (depth + 1 >= kMaxPasses) return;
+    for (int m = 7; m >= 5; --m) {
+      const int l = n - s0 - m;
+      if (l < 3 || 10 - m > l) continue;
+      cur.push_back(m);
+      rec(s0 + m, cost + (m + 1) / 2, depth + 1);
+      cur.pop_back();
+    }
+  };
+  rec(0, 0, 0);
+  return best;
+}
+
+// batch_split for every size a batch job can have, computed once.
 static const std::vector<int>& split_of(int n) {
   static const std::vector<std::vector<int>> table = [] {
     std::vector<std::vector<int>> t(kMaxLog2n + 1);
-    for (int m = 11; m <= kMaxLog2n; ++m) t[m] = engine_split(m);
+    for (int m = 11; m <= kMaxLog2n; ++m) t[m] = batch_split(m);
     return t;
   }();
   return table[n];

@@ -56,25 +56,24 @@ static_assert(sizeof(WorkItem) == 16, "work item layout");
 
 // Tile shapes of the persistent kernel (all 256 threads).  Sizes 2^1 and
 // 2^2 use unrolled one-thread tiles; every other size and both mappings run
-// on NttEngine<3> (8 elements per thread), whose code is shared by all of
-// them.  TPC = 256 / (threads per sub-transform).
+// on NttEngine<kBatchLogR> (4 elements per thread), whose code is shared by
+// all of them.  TPC = 256 / (threads per sub-transform).  Interleaved
+// (strided) tiles keep at least 8 adjacent columns (128 bytes of each row).
+constexpr int kBatchLogR = 2;
 #define BNTT_BATCH_SHAPES(X)               \
   X(0, 1, 1, 256, MAP_CONTIG)              \
   X(1, 2, 2, 256, MAP_CONTIG)              \
-  X(2, 3, 3, 256, MAP_CONTIG)              \
-  X(3, 4, 3, 128, MAP_CONTIG)              \
-  X(4, 5, 3, 64, MAP_CONTIG)               \
-  X(5, 6, 3, 32, MAP_CONTIG)               \
-  X(6, 7, 3, 16, MAP_CONTIG)               \
-  X(7, 8, 3, 8, MAP_CONTIG)                \
-  X(8, 9, 3, 4, MAP_CONTIG)                \
-  X(9, 10, 3, 2, MAP_CONTIG)               \
-  X(10, 5, 3, 64, MAP_INTERLEAVED)         \
-  X(11, 6, 3, 32, MAP_INTERLEAVED)         \
-  X(12, 7, 3, 16, MAP_INTERLEAVED)         \
-  X(13, 8, 3, 8, MAP_INTERLEAVED)          \
-  X(14, 9, 3, 4, MAP_INTERLEAVED)          \
-  X(15, 10, 3, 2, MAP_INTERLEAVED)
+  X(2, 3, 2, 128, MAP_CONTIG)              \
+  X(3, 4, 2, 64, MAP_CONTIG)               \
+  X(4, 5, 2, 32, MAP_CONTIG)               \
+  X(5, 6, 2, 16, MAP_CONTIG)               \
+  X(6, 7, 2, 8, MAP_CONTIG)                \
+  X(7, 8, 2, 4, MAP_CONTIG)                \
+  X(8, 9, 2, 2, MAP_CONTIG)                \
+  X(9, 10, 2, 1, MAP_CONTIG)               \
+  X(10, 5, 2, 32, MAP_INTERLEAVED)         \
+  X(11, 6, 2, 16, MAP_INTERLEAVED)         \
+  X(12, 7, 2, 8, MAP_INTERLEAVED)
 
 struct BatchShape {
   int m, logr, tpc, map;
@@ -209,7 +208,7 @@ __device__ __noinline__ void run_item_tiny(const WorkItem& it, const BatchArgs& 
 template <class Arith>
 __device__ __noinline__ void run_item_engine(const WorkItem& it, const BatchArgs& ba, uint4* smem,
                                              const ModParams& mp, int layout, int* s_flag) {
-  using E = NttEngine<3, Arith>;
+  using E = NttEngine<kBatchLogR, Arith>;
   int m, map;
   shape_of(it.shape, &m, &map);
   int sub, lane;

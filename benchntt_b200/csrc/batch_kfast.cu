@@ -4,6 +4,8 @@
 
 namespace bntt {
 const void* batch_kernel_fast_minb(int minb) {
-  return minb == 2 ? (const void*)&k_batch<ArithFast, 2> : (const void*)&k_batch<ArithFast, 3>;
+  return minb == 2   ? (const void*)&k_batch<ArithFast, 2>
+         : minb == 3 ? (const void*)&k_batch<ArithFast, 3>
+                     : (const void*)&k_batch<ArithFast, 4>;
 }
 }  // namespace bntt

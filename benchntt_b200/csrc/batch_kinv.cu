@@ -42,7 +42,7 @@ __device__ __noinline__ void run_item_tiny_inv(const WorkItem& it, const BatchAr
 
 __device__ __noinline__ void run_item_engine_inv(const WorkItem& it, const BatchArgs& ba, uint4* smem,
                                                  const ModParams& mp, int layout, int* s_flag) {
-  using E = NttEngine<3, ArithFast>;
+  using E = NttEngine<kBatchLogR, ArithFast>;
   int m, map;
   shape_of(it.shape, &m, &map);
   int sub, lane;
@@ -79,6 +79,6 @@ __global__ void __launch_bounds__(kBatchThreads, MINB)
 
 }  // namespace
 
-const void* batch_kernel_inverse() { return (const void*)&k_batch_inv<3>; }
+const void* batch_kernel_inverse() { return (const void*)&k_batch_inv<4>; }
 
 }  // namespace bntt

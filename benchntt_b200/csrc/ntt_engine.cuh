@@ -28,8 +28,9 @@ struct NttEngine {
     int n, base, extra;
     __device__ __forceinline__ explicit Passes(int M) {
       n = (M + LOGR - 1) / LOGR;
-      // M / n for n <= 4 and M <= 31 without a division instruction
-      base = n == 1 ? M : n == 2 ? M >> 1 : n == 3 ? (M * 11) >> 5 : M >> 2;
+      // M / n without a division instruction: n <= 4 and M <= 31, or n = 5
+      // and M <= 10 (the 4-element engine's 2^9 and 2^10)
+      base = n == 1 ? M : n == 2 ? M >> 1 : n == 3 ? (M * 11) >> 5 : n == 4 ? M >> 2 : (M * 13) >> 6;
       extra = M - base * n;
     }
     __device__ __forceinline__ int bits(int p) const { return base + (p < extra ? 1 : 0); }
@@ -211,8 +212,9 @@ struct NttEngine {
       }
       // with LOGR = 3 the balanced passes of 2^3..2^10 points have 2 or 3
       // stages, so width 1 needs no code there
-      if (r == 3)
-        pass<3, LDP, INV, EPI>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout, ep);
+      if (LOGR >= 3 && r == 3)
+        pass<(LOGR >= 3 ? 3 : 1), LDP, INV, EPI>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp,
+                                                 layout, ep);
       else if (r == 2)
         pass<2, LDP, INV, EPI>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout, ep);
       else if (LOGR != 3)

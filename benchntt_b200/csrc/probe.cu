@@ -63,17 +63,22 @@ extern "C" int bntt_probe_imad_peak(bntt_ctx* c, double* ops_per_second) {
 }
 
 // Butterfly ceiling: the kernels' own butterfly (pseudo-Mersenne multiply,
-// the reference's addmod / submod) on register-resident data, radix-8 groups
-// of 12 butterflies, at the persistent kernel's occupancy (3 CTAs of 256
-// threads per SM).  No memory traffic, no index arithmetic: the rate any NTT
-// kernel of this arithmetic can approach.
+// the reference's addmod / submod) on register-resident data, in radix-4
+// groups of 4 butterflies (the persistent kernel's 4 elements per thread), at
+// the persistent kernel's occupancy (4 CTAs of 256 threads per SM).  No
+// memory traffic, no index arithmetic: the rate any NTT kernel of this
+// arithmetic can approach.
 namespace bntt {
 
-__global__ void __launch_bounds__(256, 3) k_butterfly_probe(uint4* out, uint32_t iters, ModParams mp) {
-  U128 v[8], w[7];
+constexpr int kProbeCtasPerSm = 4;
+constexpr int kProbeButterfliesPerIter = 4;
+
+__global__ void __launch_bounds__(256, kProbeCtasPerSm) k_butterfly_probe(uint4* out, uint32_t iters,
+                                                                         ModParams mp) {
+  U128 v[4], w[3];
   uint32_t h = (blockIdx.x * 256u + threadIdx.x) * 2654435761u + 1u;
 #pragma unroll
-  for (int e = 0; e < 15; ++e) {
+  for (int e = 0; e < 7; ++e) {
     U128 t;
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
@@ -81,23 +86,18 @@ __global__ void __launch_bounds__(256, 3) k_butterfly_probe(uint4* out, uint32_t
       t.w[l] = h;
     }
     t.w[3] &= 0x07FFFFFFu;  // < 2^123 < q
-    if (e < 8) v[e] = t;
-    else w[e - 8] = t;
+    if (e < 4) v[e] = t;
+    else w[e - 4] = t;
   }
   for (uint32_t it = 0; it < iters; ++it) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) butterfly<ArithFast>(v[k], v[k + 4], w[0], mp);
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      butterfly<ArithFast>(v[k], v[k + 2], w[1], mp);
-      butterfly<ArithFast>(v[k + 4], v[k + 6], w[2], mp);
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) butterfly<ArithFast>(v[2 * k], v[2 * k + 1], w[3 + k], mp);
+    for (int k = 0; k < 2; ++k) butterfly<ArithFast>(v[k], v[k + 2], w[0], mp);
+    butterfly<ArithFast>(v[0], v[1], w[1], mp);
+    butterfly<ArithFast>(v[2], v[3], w[2], mp);
   }
   uint32_t s = 0;
 #pragma unroll
-  for (int e = 0; e < 8; ++e) s ^= v[e].w[0] ^ v[e].w[1] ^ v[e].w[2] ^ v[e].w[3];
+  for (int e = 0; e < 4; ++e) s ^= v[e].w[0] ^ v[e].w[1] ^ v[e].w[2] ^ v[e].w[3];
   if (s == 0x9E3779B9u) out[0] = make_uint4(s, 0u, 0u, 0u);  // keeps the results live
 }
 
@@ -114,8 +114,8 @@ extern "C" int bntt_probe_butterfly_peak(bntt_ctx* c, double* butterflies_per_se
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const uint32_t iters = 512;
-  const unsigned grid = (unsigned)c->sms * 3;
+  const uint32_t iters = 1536;
+  const unsigned grid = (unsigned)c->sms * kProbeCtasPerSm;
   float best = 1e30f;
   for (int rep = 0; rep < 3; ++rep) {
     cudaEventRecord(e0, c->stream);
@@ -134,7 +134,7 @@ extern "C" int bntt_probe_butterfly_peak(bntt_ctx* c, double* butterflies_per_se
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   ctx_free(c, out);
-  const double bfly = (double)grid * 256.0 * iters * 12.0;
+  const double bfly = (double)grid * 256.0 * iters * kProbeButterfliesPerIter;
   *butterflies_per_second = bfly / (best * 1e-3);
   return BNTT_OK;
 }

@@ -109,11 +109,11 @@ constexpr size_t kLaunchBytes = (size_t)256 << 20;
 
 // Staging bytes of the schedule of a launch with at most `jobs` NTTs holding
 // at most `elems` elements: every pass of a transform of 2^11 or more
-// elements has 2^n / 2048 tiles, and a small-size tile holds one job or more.
+// elements has 2^n / 1024 tiles, and a small-size tile holds one job or more.
 inline size_t schedule_bytes_bound(size_t jobs, size_t elems) {
   auto r256 = [](size_t v) { return (v + 255) & ~(size_t)255; };
   const size_t large = std::min(jobs, elems >> 11);
-  const size_t items = jobs + kMaxPasses * (elems >> 11);
+  const size_t items = jobs + kMaxPasses * (elems >> 10);
   return r256((kCtlHeader + large * kMaxPasses) * 4) + r256(large * kMaxPasses * 4) +
          r256(items * sizeof(WorkItem)) + r256(jobs * 4) + r256(jobs * sizeof(DevJob));
 }
