@@ -16,8 +16,8 @@ namespace bntt {
 const void* batch_kernel_fast_minb(int minb);
 const void* batch_kernel_ref();
 
-// Resident CTAs per SM the fast batch kernel is compiled for (2 or 3); the
-// autotuner may change it.  BNTT_BATCH_MINB overrides it at start-up.
+// Resident CTAs per SM the fast batch kernel is compiled for (2, 3 or 4,
+// default 4).  BNTT_BATCH_MINB overrides it at start-up.
 static std::atomic<int> g_batch_minb{[] {
   const char* e = getenv("BNTT_BATCH_MINB");
   const int v = e ? atoi(e) : 4;

@@ -1,5 +1,6 @@
 // batch_kfast.cu -- the persistent batch kernel with ArithFast, compiled for
-// two or three resident CTAs per SM (register budget 128 or 85 per thread).
+// two, three or four resident CTAs per SM (register budget 128, 85 or 64 per
+// thread; four is the default).
 #include "batch_dev.cuh"
 
 namespace bntt {
