@@ -17,14 +17,12 @@ const void* batch_kernel_fast_minb(int minb);
 const void* batch_kernel_ref();
 
 // Resident CTAs per SM the fast batch kernel is compiled for (2, 3 or 4,
-// default 4).  BNTT_BATCH_MINB overrides it at start-up.
-static std::atomic<int> g_batch_minb{[] {
+// default 4), read once at start-up from BNTT_BATCH_MINB.
+static const int g_batch_minb = [] {
   const char* e = getenv("BNTT_BATCH_MINB");
   const int v = e ? atoi(e) : 4;
   return v == 2 || v == 3 ? v : 4;
-}()};
-int batch_minb() { return g_batch_minb.load(std::memory_order_relaxed); }
-void set_batch_minb(int m) { g_batch_minb.store(m == 2 || m == 3 ? m : 4, std::memory_order_relaxed); }
+}();
 
 size_t shape_smem(int s) {
   const BatchShape& b = kShapes[s];
