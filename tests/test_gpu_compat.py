@@ -64,3 +64,14 @@ def test_polymul_driver(tmp_path, logn, batch):
     out = subprocess.run([exe, str(logn), str(batch)], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
     assert out.stdout.strip() == f"{1 << logn} fail: 0"
+
+
+@pytest.mark.parametrize("runs,jobs", [(1, 10), (4, 40)])
+def test_batch_host_driver(tmp_path, runs, jobs):
+    """A C program on the native ABI: mixed-size host-buffer batches queued
+    back to back (bntt_batch_run_host_async, one bntt_batch_sync), every job
+    equal to the plan's single-transform host call."""
+    exe = build(tmp_path, "batch_host_driver.c")
+    out = subprocess.run([exe, str(runs), str(jobs)], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.strip() == "fail: 0"
