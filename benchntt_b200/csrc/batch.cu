@@ -158,30 +158,45 @@ static const std::vector<int>& split_of(int n) {
 int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count,
                    bool inverse) {
   sc.djobs.resize(count);
+  sc.job_log2n.resize(count);
+  sc.large.clear();
   sc.items.clear();
   sc.pass_tiles.clear();
   sc.nslots = 0;
-  // one pass over the jobs: descriptors, the count of small jobs per size
+  // the plans' fields, looked up once instead of per job
+  const size_t np = b->plans.size();
+  sc.plan_tw.resize(np);
+  sc.plan_log2n.resize(np);
+  for (size_t k = 0; k < np; ++k) {
+    sc.plan_tw[k] = static_cast<const uint4*>(inverse ? b->plans[k]->tw_inv : b->plans[k]->tw);
+    sc.plan_log2n[k] = (uint8_t)b->plans[k]->log2n;
+  }
+  // one pass over the jobs: descriptors, sizes, small jobs counted per size
   uint32_t per_size[11] = {};
+  const uint4* const* tw = sc.plan_tw.data();
+  const uint8_t* plog = sc.plan_log2n.data();
   for (size_t i = 0; i < count; ++i) {
     const bntt_job& jb = jobs[i];
-    BNTT_REQUIRE(jb.plan < b->plans.size(), "job %zu: plan index %u out of range", i, jb.plan);
+    BNTT_REQUIRE(jb.plan < np, "job %zu: plan index %u out of range", i, jb.plan);
     BNTT_REQUIRE(jb.x && jb.y, "job %zu: NULL buffer", i);
     BNTT_REQUIRE((((uintptr_t)jb.x | (uintptr_t)jb.y) & 15) == 0, "job %zu: buffers must be 16-byte aligned", i);
-    const bntt_plan* p = b->plans[jb.plan];
+    const uint32_t n = plog[jb.plan];
     DevJob& d = sc.djobs[i];
     d.x = static_cast<const uint4*>(jb.x);
     d.y = static_cast<uint4*>(jb.y);
-    d.tw = static_cast<const uint4*>(inverse ? p->tw_inv : p->tw);
-    d.log2n = p->log2n;
-    if (p->log2n <= 10) {
+    d.tw = tw[jb.plan];
+    d.log2n = n;
+    sc.job_log2n[i] = (uint8_t)n;
+    if (n <= 10) {
       d.slot = 0;
-      ++per_size[p->log2n];
+      ++per_size[n];
     } else {
       d.slot = (uint32_t)sc.nslots++;
+      sc.large.push_back((uint32_t)i);
     }
   }
-  // small jobs in size order, largest size first (a counting sort)
+  // small jobs in size order, largest size first (a counting sort over the
+  // compact size array)
   uint32_t first[11] = {}, fill[11];
   uint32_t small = 0;
   for (int n = 10; n >= 1; --n) {
@@ -190,15 +205,15 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
   }
   std::copy(first, first + 11, fill);
   sc.order.resize(small);
+  const uint8_t* sizes = sc.job_log2n.data();
   for (size_t i = 0; i < count; ++i) {
-    const uint32_t n = sc.djobs[i].log2n;
+    const uint32_t n = sizes[i];
     if (n <= 10) sc.order[fill[n]++] = (uint32_t)i;
   }
   for (auto& l : sc.later) l.clear();
   sc.pass_tiles.assign(sc.nslots * kMaxPasses, 0);
-  for (size_t ji = 0; ji < count; ++ji) {
+  for (const uint32_t ji : sc.large) {
     const DevJob& d = sc.djobs[ji];
-    if (d.log2n <= 10) continue;
     const int n = (int)d.log2n;
     const std::vector<int>& passes = split_of(n);
     BNTT_REQUIRE(!passes.empty() && passes.size() <= (size_t)kMaxPasses, "log2n %d needs too many passes", n);

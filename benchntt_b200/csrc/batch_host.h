@@ -19,6 +19,10 @@ struct Schedule {
   std::vector<WorkItem> items;
   std::vector<uint32_t> pass_tiles;
   std::vector<WorkItem> later[kMaxPasses];  // build scratch: pass items by run position
+  std::vector<uint8_t> job_log2n;           // build scratch: each job's size
+  std::vector<uint32_t> large;              // build scratch: jobs above 2^10 points
+  std::vector<const uint4*> plan_tw;        // build scratch: the plans' tables
+  std::vector<uint8_t> plan_log2n;
   size_t nslots = 0;
   // device copies of djobs, order, items and pass_tiles in one buffer, two
   // buffers used in turn: a new job list is copied into the one the running
