@@ -481,6 +481,7 @@ int bntt_batch_run_dev(bntt_batch* b, const bntt_job* jobs, size_t count) {
   BNTT_REQUIRE(b && (jobs || count == 0), "NULL argument");
   if (int rc = ctx_use_device(b->ctx)) return rc;
   b->last_launches = 0;
+  b->noalloc_err = nullptr;
   if (count == 0) return BNTT_OK;
   const bool inject = b->inject_polls != 0;
   const bool same = !inject && b->last_jobs.size() == count && b->main.stream == b->ctx->stream &&
@@ -503,6 +504,7 @@ int bntt_batch_run_inverse_dev(bntt_batch* b, const bntt_job* jobs, size_t count
   BNTT_REQUIRE(b && (jobs || count == 0), "NULL argument");
   if (int rc = ctx_use_device(b->ctx)) return rc;
   b->last_launches = 0;
+  b->noalloc_err = nullptr;
   if (count == 0) return BNTT_OK;
   BNTT_REQUIRE(b->fast, "the inverse transform needs q = 2^124 - k (k < 2^31), mu = floor(2^251/q) "
                "and the default arithmetic");
@@ -527,6 +529,12 @@ int bntt_batch_status(bntt_batch* b) {
   BNTT_CK(cudaStreamSynchronize(b->ctx->stream));
   destroy_retired(b->main);
   destroy_retired(b->inv);
+  if (b->noalloc_err) {  // the latest run used the shared no-allocation array
+    uint32_t err = 0;
+    BNTT_CK(cudaMemcpy(&err, b->noalloc_err, 4, cudaMemcpyDeviceToHost));
+    if (err) return set_error(BNTT_ETIMEOUT, "a pass of a large transform waited too long for its predecessor");
+    return BNTT_OK;
+  }
   if (int rc = schedule_status(b->main)) return rc;
   if (int rc = schedule_status(b->inv)) return rc;
   for (Schedule& s : b->groups)
@@ -571,6 +579,7 @@ int bntt_batch_run_host_async(bntt_batch* b, const bntt_job* jobs, size_t count)
   bntt_ctx* c = b->ctx;
   if (int rc = ctx_use_device(c)) return rc;
   b->last_launches = 0;
+  b->noalloc_err = nullptr;
   if (count == 0) return BNTT_OK;
   cudaStream_t s_in = c->copy_stream[0], s_out = c->copy_stream[1], s_run = c->stream;
   const bool inject = b->inject_polls != 0;
@@ -771,6 +780,7 @@ extern "C" int bntt_batch_run_percall_dev(bntt_batch* b, const bntt_job* jobs, s
   BNTT_REQUIRE(b && (jobs || count == 0), "NULL argument");
   if (int rc = ctx_use_device(b->ctx)) return rc;
   b->last_launches = 0;
+  b->noalloc_err = nullptr;
   const uint64_t before = b->ctx->launches;
   for (size_t i = 0; i < count; ++i) {
     BNTT_REQUIRE(jobs[i].plan < b->plans.size(), "job %zu: plan index out of range", i);
@@ -796,10 +806,6 @@ namespace bntt {
 constexpr size_t kNoAllocScratchBytes = 4u << 20;  // 4 MiB on every GPU that loads the library
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kNoAllocMaxDevices = 64;
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_base[kNoAllocMaxDevices] = {};
-
 static size_t round256(size_t v) { return (v + 255) & ~(size_t)255; }
 
 }  // namespace bntt
@@ -808,20 +814,29 @@ extern "C" int bntt_batch_run_dev_noalloc(bntt_batch* b, const bntt_job* jobs, s
   BNTT_REQUIRE(b && (jobs || count == 0), "NULL argument");
   bntt_ctx* c = b->ctx;
   if (int rc = ctx_use_device(c)) return rc;
-  BNTT_REQUIRE(c->device < kNoAllocMaxDevices, "device %d beyond the supported range", c->device);
+  b->last_launches = 0;
+  b->noalloc_err = nullptr;
+  // The schedule is copied from host vectors that are freed when this call
+  // returns; captured into a graph, those copies would read freed memory at
+  // every replay.  Checked before any other CUDA call, so a refused call
+  // leaves the capture intact.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  BNTT_CK(cudaStreamIsCapturing(c->stream, &cap));
+  BNTT_REQUIRE(cap == cudaStreamCaptureStatusNone,
+               "bntt_batch_run_dev_noalloc cannot run while its stream is being captured");
   if (count == 0) return BNTT_OK;
-  // Once per device, with that device current: the device address of the
+  // Once per context, with its device current: the device address of the
   // array (its name is only a host-side stand-in in host code).
   void* base = nullptr;
   {
-    std::lock_guard<std::mutex> g(g_noalloc_mu);
-    if (!g_noalloc_base[c->device]) {
+    std::lock_guard<std::mutex> g(c->mu);
+    if (!c->noalloc_base) {
       void* p = nullptr;
       cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(no-alloc scratch)");
-      g_noalloc_base[c->device] = p;
+      c->noalloc_base = p;
     }
-    base = g_noalloc_base[c->device];
+    base = c->noalloc_base;
   }
   Schedule sc;  // host-side vectors only
   if (int rc = build_schedule(b, sc, jobs, count)) return rc;
@@ -840,6 +855,7 @@ extern "C" int bntt_batch_run_dev_noalloc(bntt_batch* b, const bntt_job* jobs, s
   // the array keeps the previous call's contents: the control words (queue
   // head, error word, pass counters) must start at zero
   BNTT_CK(cudaMemsetAsync(s + o_ctl, 0, cb, st));
+  b->noalloc_err = reinterpret_cast<const uint32_t*>(s + o_ctl) + 1;
   if (pb) BNTT_CK(cudaMemcpyAsync(s + o_pt, sc.pass_tiles.data(), pb, cudaMemcpyHostToDevice, st));
   if (ib) BNTT_CK(cudaMemcpyAsync(s + o_it, sc.items.data(), ib, cudaMemcpyHostToDevice, st));
   if (ob) BNTT_CK(cudaMemcpyAsync(s + o_or, sc.order.data(), ob, cudaMemcpyHostToDevice, st));

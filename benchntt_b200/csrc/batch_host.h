@@ -77,6 +77,9 @@ struct bntt_batch {
   bool host_inflight = false;        // host runs not yet passed to bntt_batch_sync
   bool host_err_pending = false;     // an error of runs finished before a rebuild
   size_t last_launches = 0;
+  // the latest run was bntt_batch_run_dev_noalloc: bntt_batch_status reads
+  // the error word it left in the shared no-allocation array
+  const uint32_t* noalloc_err = nullptr;
   // fault injection for tests of the failure path (bntt_batch_inject_wait_timeout)
   uint32_t inject_polls = 0;
   // inverse runs (bntt_batch_run_inverse_dev)

@@ -111,6 +111,10 @@ struct bntt_ctx {
   size_t stage_bytes = 0;
   cudaStream_t copy_stream[2] = {nullptr, nullptr};
   cudaEvent_t ev[8] = {};
+  // device address of the no-allocation scratch array, looked up by the
+  // context's first bntt_batch_run_dev_noalloc call (a context created after
+  // a device reset looks it up again)
+  void* noalloc_base = nullptr;
   std::mutex mu;
 };
 

@@ -246,16 +246,20 @@ int bntt_batch_run_inverse_dev(bntt_batch *batch, const bntt_job *jobs, size_t c
  * Its scratch (work items, job descriptors, control words) lives in one
  * 4 MiB array inside the library, present on every GPU that loads it until
  * the process exits; a job list whose schedule needs more (roughly 70,000
- * transforms) is rejected with BNTT_EINVAL.  The first call on a device looks
- * up that array's device address; make that first call before any stream
- * capture.  Every call reuses the same array: the control words are cleared
- * on each call, and calls whose work overlaps on the GPU (several streams,
- * contexts or threads on one device) race -- serialise them.  Asynchronous on
- * the context's stream; a device-side wait that gives up is not reported
- * here (use bntt_batch_run_dev when that check is needed). */
+ * transforms) is rejected with BNTT_EINVAL.  The first call through a context
+ * looks up that array's device address (again for a context created after a
+ * device reset).  The schedule is copied from host memory that is released
+ * when the call returns, so the call is refused with BNTT_EINVAL while the
+ * context's stream is being captured into a CUDA graph.  Every call reuses
+ * the same array: the control words are cleared on each call, and calls whose
+ * work overlaps on the GPU (several streams, contexts or threads on one
+ * device) race -- serialise them.  Asynchronous on the context's stream. */
 int bntt_batch_run_dev_noalloc(bntt_batch *batch, const bntt_job *jobs, size_t count);
-/* Status of the last run: BNTT_OK, or BNTT_ETIMEOUT if a device-side wait
- * gave up (synchronises the stream). */
+/* Status of the batch's latest run: BNTT_OK, or BNTT_ETIMEOUT if a
+ * device-side wait gave up (synchronises the stream).  After
+ * bntt_batch_run_dev_noalloc it reads the error word that run left in the
+ * shared array, so read it before another no-allocation call on the same
+ * device reuses the array. */
 int bntt_batch_status(bntt_batch *batch);
 /* Fault injection for tests of the failure path: the next
  * bntt_batch_run_dev makes the waits of later HBM passes unreachable and gives
