@@ -155,6 +155,8 @@ _SIGS = [
     ("bntt_server_get_stats", _I, [_P, ctypes.POINTER(ServerStatsC)]),
     ("bntt_server_replay", _I, [_P, ctypes.POINTER(RequestC), _S, _I,
                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    ("bntt_server_replay_ex", _I, [_P, ctypes.POINTER(RequestC), _S, _I, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     ("bntt_autotune", _I, [_P, ctypes.c_char_p]),
     ("bntt_autotune_load", _I, [_P, ctypes.c_char_p]),
     ("bntt_autotune_reset", _I, []),
@@ -497,13 +499,20 @@ class Server:
         check(lib().bntt_server_get_stats(self._h, ctypes.byref(st)))
         return {f: getattr(st, f) for f, _ in ServerStatsC._fields_}
 
-    def replay(self, reqs, serial: bool = False):
-        """Latencies (s) of every request and the wall time of the replay."""
+    def replay(self, reqs, serial: bool = False, service: bool = False):
+        """Latencies (s) of every request and the wall time of the replay;
+        with service=True also each request's service time (completion less
+        admission), as (latency, service, wall)."""
         n = len(reqs)
         lat = (ctypes.c_double * n)()
+        svc = (ctypes.c_double * n)() if service else None
         wall = ctypes.c_double()
-        check(lib().bntt_server_replay(self._h, reqs, n, 1 if serial else 0, lat, ctypes.byref(wall)))
-        return np.frombuffer(lat, dtype=np.float64).copy(), wall.value
+        check(lib().bntt_server_replay_ex(self._h, reqs, n, 1 if serial else 0, lat, svc,
+                                          ctypes.byref(wall)))
+        lat_a = np.frombuffer(lat, dtype=np.float64).copy()
+        if service:
+            return lat_a, np.frombuffer(svc, dtype=np.float64).copy(), wall.value
+        return lat_a, wall.value
 
     def close(self) -> None:
         if self._h:

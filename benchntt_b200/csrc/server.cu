@@ -462,6 +462,11 @@ int bntt_server_get_stats(bntt_server* s, bntt_server_stats* st) {
 
 int bntt_server_replay(bntt_server* s, const bntt_request* reqs, size_t n, int serial,
                        double* latency_s, double* wall_s) {
+  return bntt_server_replay_ex(s, reqs, n, serial, latency_s, nullptr, wall_s);
+}
+
+int bntt_server_replay_ex(bntt_server* s, const bntt_request* reqs, size_t n, int serial,
+                          double* latency_s, double* service_s, double* wall_s) {
   BNTT_REQUIRE(s && (reqs || n == 0) && latency_s && wall_s, "NULL argument");
   if (n == 0) {
     *wall_s = 0;
@@ -488,6 +493,7 @@ int bntt_server_replay(bntt_server* s, const bntt_request* reqs, size_t n, int s
       const double t_arr = base + r.t_arrive;
       while (s->now() < t_arr) {
       }
+      const double t_start = s->now();  // the call begins: its admission
       if (r.kind == BNTT_REQ_NTT) {
         rc = ntt_forward_on(s->engine->plans[r.plan], y, r.x, 1, s->ctx->stream);
       } else {
@@ -501,6 +507,7 @@ int bntt_server_replay(bntt_server* s, const bntt_request* reqs, size_t n, int s
       }
       last_done = s->now();
       latency_s[i] = last_done - t_arr;
+      if (service_s) service_s[i] = last_done - t_start;
     }
     {
       std::lock_guard<std::mutex> g(s->mu);
@@ -518,7 +525,10 @@ int bntt_server_replay(bntt_server* s, const bntt_request* reqs, size_t n, int s
     bntt_server_poll(s, got.data(), got.size(), &k);
     for (size_t j = 0; j < k; ++j) {
       const bntt_completion& cpl = got[j];
-      if (cpl.tag < n) latency_s[cpl.tag] = cpl.t_done - cpl.t_arrive;
+      if (cpl.tag < n) {
+        latency_s[cpl.tag] = cpl.t_done - cpl.t_arrive;
+        if (service_s) service_s[cpl.tag] = cpl.t_done - cpl.t_admit;
+      }
       if (cpl.status && !rc) rc = cpl.status;
       last_done = std::max(last_done, cpl.t_done);
       bntt_server_release(s, cpl.y);

@@ -371,6 +371,11 @@ int bntt_server_get_stats(bntt_server *srv, bntt_server_stats *stats);
  * released as they complete. */
 int bntt_server_replay(bntt_server *srv, const bntt_request *reqs, size_t n, int serial,
                        double *latency_s, double *wall_s);
+/* The same, also returning each request's service time in `service_s` (may
+ * be NULL): completion less admission, i.e. the latency without the time
+ * spent queued before it was admitted (serial: before its call began). */
+int bntt_server_replay_ex(bntt_server *srv, const bntt_request *reqs, size_t n, int serial,
+                          double *latency_s, double *service_s, double *wall_s);
 
 /* ------------------------------------------------------------- autotuner */
 /* Times every compiled kernel shape for transform sizes 2^1..2^10 (register

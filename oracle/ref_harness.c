@@ -254,6 +254,162 @@ static void ntt_range(void *vctx, size_t b, size_t e)
 #endif
 }
 
+/* Per-transform entry points for a whole mixed-size batch run by
+ * oracle/ref_batch.c, one shared object per size:
+ *   bntt_ref_prep(T, q, mu)      the size's table in the form ntt() reads,
+ *                                built once per size (the table expansion
+ *                                ntt_pre performs, src/ntt_avx512.c:386-441,
+ *                                src/ntt_avx2.c:507-552), before any timing
+ *   bntt_ref_scratch_new/free    one thread's working arrays for ntt()
+ *   bntt_ref_ntt_only(prep, scratch, x, y)
+ *                                ntt() alone: the reference drivers' timed
+ *                                region (src/ntt_avx512.c:585-590,
+ *                                src/ntt_avx2.c:713-718, src/ntt_scalar.c:
+ *                                670-676).  SIMD: x is the packed input
+ *                                ntt_pre leaves in tempx, which is the pair
+ *                                array itself, and y receives `as`, which is
+ *                                the output pair array ntt_post stores
+ *                                (both 64-byte aligned).  Scalar: x and y are
+ *                                native uint128_t arrays.
+ *   bntt_ref_ntt_full(T, q, mu, scratch, x, y)
+ *                                the whole per-call sequence on hi-first
+ *                                pairs: ntt_pre + ntt + ntt_post (SIMD), or
+ *                                the pair conversions around ntt() (scalar). */
+struct ref_prep {
+#if defined(REF_IMPL_SCALAR)
+    uint128_t *tw;
+#else
+    vec *twdh, *twdl;
+    vec mh, ml, muh, mul, ph, pl;
+#endif
+    uint128_t m, mu;
+};
+
+struct ref_scratch {
+#if defined(REF_IMPL_SCALAR)
+    uint128_t *x, *y, *tw, *as0, *as1;
+#else
+    vec *twdh, *twdl, *tempx, *as, *xh, *xl, *ash, *asl, *th, *tl;
+#endif
+};
+
+/* Sets the SIMD constants the reference's main() sets; call once per shared
+ * object before any thread uses it. */
+void bntt_ref_init(void) { ref_init(); }
+
+void *bntt_ref_scratch_new(void)
+{
+    const size_t n = REF_N;
+    struct ref_scratch *s = calloc(1, sizeof *s);
+#if defined(REF_IMPL_SCALAR)
+    s->x = xalloc(n * 16); s->y = xalloc(n * 16); s->tw = xalloc(n * 16);
+    s->as0 = xalloc(n * 16); s->as1 = xalloc(n * 16);
+#else
+    const size_t ops = n / (2 * LANES), v = n / LANES;
+    s->twdh = xalloc(sizeof(vec) * REF_STAGES * ops); s->twdl = xalloc(sizeof(vec) * REF_STAGES * ops);
+    s->tempx = xalloc(sizeof(vec) * (2 * n / LANES)); s->as = xalloc(sizeof(vec) * (2 * n / LANES));
+    s->xh = xalloc(sizeof(vec) * v); s->xl = xalloc(sizeof(vec) * v);
+    s->ash = xalloc(sizeof(vec) * v); s->asl = xalloc(sizeof(vec) * v);
+    s->th = xalloc(sizeof(vec) * v); s->tl = xalloc(sizeof(vec) * v);
+#endif
+    return s;
+}
+
+void bntt_ref_scratch_free(void *p)
+{
+    struct ref_scratch *s = p;
+    if (!s) return;
+#if defined(REF_IMPL_SCALAR)
+    free(s->x); free(s->y); free(s->tw); free(s->as0); free(s->as1);
+#else
+    free(s->twdh); free(s->twdl); free(s->tempx); free(s->as); free(s->xh); free(s->xl);
+    free(s->ash); free(s->asl); free(s->th); free(s->tl);
+#endif
+    free(s);
+}
+
+void *bntt_ref_prep(const uint64_t *T, uint64_t mh, uint64_t ml, uint64_t muh, uint64_t mul)
+{
+    const size_t n = REF_N;
+    struct ref_prep *p = xalloc(sizeof *p);  /* holds vectors: 64-byte aligned */
+    p->m = MK(mh, ml);
+    p->mu = MK(muh, mul);
+#if defined(REF_IMPL_SCALAR)
+    p->tw = xalloc(n * 16);
+    for (size_t i = 0; i < n; ++i) p->tw[i] = MK(T[2 * i], T[2 * i + 1]);
+#else
+    ref_init();
+    const size_t ops = n / (2 * LANES);
+    p->twdh = xalloc(sizeof(vec) * REF_STAGES * ops);
+    p->twdl = xalloc(sizeof(vec) * REF_STAGES * ops);
+    vec *tempx = xalloc(sizeof(vec) * (2 * n / LANES));
+    uint64_t *x0 = xalloc(n * 16);
+#if defined(REF_IMPL_AVX2)
+    ntt_pre(x0, (uint64_t *)T, p->m, p->mu, tempx, p->twdh, p->twdl, &p->mh, &p->ml, &p->muh, &p->mul);
+#else
+    ntt_pre(x0, (uint64_t *)T, p->m, p->mu, tempx, p->twdh, p->twdl, &p->mh, &p->ml, &p->muh, &p->mul,
+            &p->ph, &p->pl);
+#endif
+    free(tempx);
+    free(x0);
+#endif
+    return p;
+}
+
+void bntt_ref_prep_free(void *vp)
+{
+    struct ref_prep *p = vp;
+    if (!p) return;
+#if defined(REF_IMPL_SCALAR)
+    free(p->tw);
+#else
+    free(p->twdh); free(p->twdl);
+#endif
+    free(p);
+}
+
+void bntt_ref_ntt_only(void *vp, void *vs, const uint64_t *x, uint64_t *y)
+{
+    struct ref_prep *p = vp;
+    struct ref_scratch *s = vs;
+#if defined(REF_IMPL_SCALAR)
+    ntt((uint128_t *)y, (uint128_t *)x, p->m, p->mu, p->tw, s->as0, s->as1);
+#elif defined(REF_IMPL_AVX2)
+    ntt((vec *)x, p->twdh, p->twdl, p->mh, p->ml, p->muh, p->mul, s->xh, s->xl, s->ash, s->asl, s->th,
+        s->tl, (vec *)y);
+#else
+    ntt((vec *)x, p->twdh, p->twdl, p->mh, p->ml, p->muh, p->mul, p->ph, p->pl, s->xh, s->xl, s->ash,
+        s->asl, s->th, s->tl, (vec *)y);
+#endif
+}
+
+void bntt_ref_ntt_full(const uint64_t *T, uint64_t mh, uint64_t ml, uint64_t muh, uint64_t mul,
+                       void *vs, const uint64_t *xs, uint64_t *ys)
+{
+    struct ref_scratch *s = vs;
+    const size_t n = REF_N;
+    const uint128_t m = MK(mh, ml), mu = MK(muh, mul);
+#if defined(REF_IMPL_SCALAR)
+    for (size_t i = 0; i < n; ++i) s->tw[i] = MK(T[2 * i], T[2 * i + 1]);
+    for (size_t i = 0; i < n; ++i) s->x[i] = MK(xs[2 * i], xs[2 * i + 1]);
+    ntt(s->y, s->x, m, mu, s->tw, s->as0, s->as1);
+    for (size_t i = 0; i < n; ++i) { ys[2 * i] = (uint64_t)(s->y[i] >> 64); ys[2 * i + 1] = (uint64_t)s->y[i]; }
+#else
+    vec vmh, vml, vmuh, vmul;
+#if defined(REF_IMPL_AVX2)
+    ntt_pre((uint64_t *)xs, (uint64_t *)T, m, mu, s->tempx, s->twdh, s->twdl, &vmh, &vml, &vmuh, &vmul);
+    ntt(s->tempx, s->twdh, s->twdl, vmh, vml, vmuh, vmul, s->xh, s->xl, s->ash, s->asl, s->th, s->tl, s->as);
+#else
+    vec ph, pl;
+    ntt_pre((uint64_t *)xs, (uint64_t *)T, m, mu, s->tempx, s->twdh, s->twdl, &vmh, &vml, &vmuh, &vmul,
+            &ph, &pl);
+    ntt(s->tempx, s->twdh, s->twdl, vmh, vml, vmuh, vmul, ph, pl, s->xh, s->xl, s->ash, s->asl, s->th,
+        s->tl, s->as);
+#endif
+    ntt_post(ys, s->as);
+#endif
+}
+
 /* `batch` contiguous transforms of N = 2^REF_STAGES hi-first pairs sharing
  * table T; each transform is the reference's full per-call sequence
  * (scalar: ntt(); SIMD: ntt_pre + ntt + ntt_post). */
