@@ -22,6 +22,8 @@
 #ifndef BNTT_COMPAT_SIMD_H
 #define BNTT_COMPAT_SIMD_H
 
+#include <string.h>
+
 #define BNTT_COMPAT_NO_MACROS
 #include "bntt_compat.h"
 #undef BNTT_COMPAT_NO_MACROS
@@ -37,8 +39,16 @@
 #define BNTT_LAST_16_(...) BNTT_ARG16_(__VA_ARGS__, 0)
 #define BNTT_LAST_(...) BNTT_CAT_(BNTT_LAST_, BNTT_CAT_(BNTT_NARGS_(__VA_ARGS__), _))(__VA_ARGS__)
 
-/* first 64-bit lane of a vector value, as an unsigned integer */
-#define BNTT_LANE0_(v) (*(const uint64_t *)&(v))
+/* first 64-bit lane of a vector value, as an unsigned integer (copied out
+ * with memcpy: reading a vector object through a uint64_t pointer would break
+ * the aliasing rules) */
+static inline uint64_t bntt_compat_lane0_(const void *p)
+{
+    uint64_t r;
+    memcpy(&r, p, sizeof r);
+    return r;
+}
+#define BNTT_LANE0_(v) (__extension__({ __typeof__(v) bntt_v_ = (v); bntt_compat_lane0_(&bntt_v_); }))
 #define BNTT_U128_(hi, lo) (((bntt_uint128)BNTT_LANE0_(hi) << 64) | (bntt_uint128)BNTT_LANE0_(lo))
 
 /* arguments that are not used are named in an unevaluated sizeof only */

@@ -44,8 +44,11 @@ def test_compat_headers_compile_as_c():
     """The reference's C drivers compile against the compat headers."""
     for src, extra in (("ntt_scalar_driver.c", ["-Dstages=8"]),
                        ("ntt_simd_driver.c", ["-Dstages=8", "-mavx2"]),
-                       ("blas_driver.c", [])):
-        subprocess.run(["gcc", "-std=gnu11", "-Wall", "-Werror", "-fsyntax-only", *extra, "-I",
+                       ("ntt_avx512_driver.c", ["-Dstages=8", "-mavx512f", "-mavx512dq"]),
+                       ("blas_driver.c", []),
+                       ("blas_simd_driver.c", ["-mavx2"]),
+                       ("blas_simd_driver.c", ["-mavx512f", "-mavx512dq", "-DBNTT_DRIVER_AVX512"])):
+        subprocess.run(["gcc", "-std=gnu11", "-O2", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", *extra, "-I",
                         os.path.join(C.ROOT, "include"),
                         os.path.join(C.ROOT, "tests", "compat", src)], check=True)
 

@@ -48,6 +48,49 @@ def test_simd_ntt_driver(tmp_path, datadir, stages):
     assert out.stdout.strip() == f"{1 << stages} fail: 0"
 
 
+def host_has(*flags) -> bool:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("flags"):
+                have = set(line.split(":", 1)[1].split())
+                return all(f in have for f in flags)
+    except OSError:
+        pass
+    return False
+
+
+AVX512 = ("-mavx512f", "-mavx512dq")
+needs_avx512 = pytest.mark.skipif(not host_has("avx512f", "avx512dq"), reason="host CPU lacks AVX-512F/DQ")
+
+
+@needs_avx512
+@pytest.mark.parametrize("stages", [4, 7, 10])
+def test_avx512_ntt_driver(tmp_path, datadir, stages):
+    """The 8-lane driver's call shape: ntt_pre with the permutation vectors,
+    the 16-argument ntt (src/ntt_avx512.c:461, driver :580-594)."""
+    exe = build(tmp_path, "ntt_avx512_driver.c", (f"-Dstages={stages}", *AVX512))
+    out = subprocess.run([exe, datadir], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.strip() == f"{1 << stages} fail: 0"
+
+
+@pytest.mark.parametrize("isa", ["avx2", "avx512"])
+def test_simd_blas_driver(tmp_path, datadir, isa):
+    """vector_add(c, a, b, mh, ml) ... axpy(c, a, b, xh, xl, mh, ml, muh, mul)
+    on __m256i / __m512i arrays (src/blas_avx2.c:448-523,
+    src/blas_avx512.c:401-476)."""
+    if isa == "avx512" and not host_has("avx512f", "avx512dq"):
+        pytest.skip("host CPU lacks AVX-512F/DQ")
+    if isa == "avx2" and not host_has("avx2"):
+        pytest.skip("host CPU lacks AVX2")
+    flags = (*AVX512, "-DBNTT_DRIVER_AVX512") if isa == "avx512" else ("-mavx2",)
+    exe = build(tmp_path, "blas_simd_driver.c", flags)
+    out = subprocess.run([exe, datadir], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.split() == ["vvadd", "fail:", "0", "vvsub", "fail:", "0", "vvmul", "fail:",
+                                  "0", "axpy", "fail:", "0"]
+
+
 def test_blas_driver(tmp_path, datadir):
     exe = build(tmp_path, "blas_driver.c")
     out = subprocess.run([exe, datadir], capture_output=True, text=True, timeout=120)
