@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0,
                     help="fraction of the uneven batch (profiling captures of a smaller case)")
+    ap.add_argument("--split", action="store_true",
+                    help="under torchrun: split one job list over the ranks by cost (strong "
+                         "scaling) instead of one whole batch per rank (weak scaling)")
     ap.add_argument("--headline-only", action="store_true",
                     help="only the persistent-kernel step (for profiler launch lists)")
     ap.add_argument("--only", choices=["uniform", "inverse", "inverse_batch", "blas", "serving"], default=None,
@@ -279,6 +282,13 @@ def run_ours(args, dist: Dist):
         n_small = max(1, int(100_000 * args.scale))
         large = tuple((l, max(1, int(c * args.scale))) for l, c in ((16, 64), (20, 4)))
         batch = W.uneven_batch(n_small=n_small, large=large)
+    split = args.split and dist.world > 1
+    # units of work one step does over the whole job: every rank's batch, or
+    # (split) the one job list the ranks share
+    units = batch.count if split else batch.count * dist.world
+    if split:   # this rank's share of the job list, longest first to the least-loaded rank
+        from benchntt_b200.dist import shard_by_cost
+        batch = W.make_batch(batch.logns[shard_by_cost(batch.logns, dist.world)[dist.rank]])
     mod = bn.modulus(Q_NTT, MU_NTT)
     plans = {n: bn.Plan(ctx, n, Q_NTT, MU_NTT,
                         bn.fill_uniform(W.SEED_TWIDDLE_BASE + n, 1 << n, Q_NTT))
@@ -314,7 +324,7 @@ def run_ours(args, dist: Dist):
     gpu_launches = ctx.launches - launches0
     ms_local = e0.elapsed_time(e1) / args.steps
     ms = dist.max(ms_local)
-    value = batch.count * dist.world / (ms * 1e-3)
+    value = units / (ms * 1e-3)
 
     # roofline of the persistent kernel (one launch per step)
     bfly = batch.butterflies
@@ -342,10 +352,12 @@ def run_ours(args, dist: Dist):
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "higher_is_better": True, "scaling": "strong" if split else "weak", "vs_baseline": None,
         "dtype": "u128 (4 x u32 limbs, exact integer)",
         "data": "synthetic: seeded uniform residues in [0, q) and seeded per-size twiddle tables",
-        "config": workload_config(dist.world, args.scale),
+        "config": dict(workload_config(dist.world, args.scale),
+                       **({"parallelism": f"dp{dist.world}: one job list split by cost over the devices"}
+                          if split else {})),
         "launch": "one CUDA-graph launch of the persistent kernel per step",
         "gpu_launches": gpu_launches,
         "roofline": roofline,
@@ -358,11 +370,11 @@ def run_ours(args, dist: Dist):
         return result, ctx
 
     # ------------------------------------------------------------ e2e (host)
-    result["e2e"] = e2e_uneven(args, dist, ctx, engine, batch, pid)
+    result["e2e"] = e2e_uneven(args, dist, ctx, engine, batch, pid, units)
     # ------------------------------------------- a new job list every step
     result["new_job_list_each_step"] = fresh_lists(args, ctx, stream, engine, jobs, batch, value)
     # ---------------------------------------------------------- per-call path
-    result["per_call"] = per_call(args, dist, ctx, stream, engine, jobs, batch, value)
+    result["per_call"] = per_call(args, dist, ctx, stream, engine, jobs, units, value)
     # ------------------------------------- one transform of N = 1024 per call
     result["single_ntt_1024"] = single_ntt(args, ctx, stream)
     # ----------------------------------------------------------------- BLAS
@@ -404,7 +416,7 @@ def measured_peaks() -> dict:
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "from_file": False}
 
 
-def e2e_uneven(args, dist, ctx, engine, batch, pid) -> dict:
+def e2e_uneven(args, dist, ctx, engine, batch, pid, units: int) -> dict:
     """The uneven batch from pinned host buffers: every step copies all
     inputs in and all outputs out (queued steps, and one call at a time)."""
     import torch
@@ -440,11 +452,11 @@ def e2e_uneven(args, dist, ctx, engine, batch, pid) -> dict:
     nbytes = batch.total * 16
     link = pcie_both_ways(xh, yh)
     del xh, yh
-    return {"value": batch.count * dist.world / dt, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+    return {"value": units / dt, "unit": UNIT, "h2d_bytes_per_step": nbytes,
             "d2h_bytes_per_step": nbytes, "ms_per_step": dt * 1e3, "steps": steps,
             "api": "bntt_batch_run_host_async per step, back to back, then bntt_batch_sync "
                    "(pinned host buffers; every step copies all inputs in and all outputs out)",
-            "one_call_at_a_time": {"value": batch.count * dist.world / dt_sync, "ms_per_step": dt_sync * 1e3,
+            "one_call_at_a_time": {"value": units / dt_sync, "ms_per_step": dt_sync * 1e3,
                                    "api": "bntt_batch_run_host (synchronous) per step"},
             "pcie_gbs_each_way": nbytes / dt / 1e9,
             "pcie_peak_gbs_each_way": link,
@@ -550,7 +562,7 @@ def fresh_lists(args, ctx, stream, engine, jobs, batch, batched_value) -> dict:
             "host_wall_ms_per_step": wall * 1e3, "vs_same_list": batch.count / (ms * 1e-3) / batched_value}
 
 
-def per_call(args, dist, ctx, stream, engine, jobs, batch, batched_value) -> dict:
+def per_call(args, dist, ctx, stream, engine, jobs, units, batched_value) -> dict:
     """The same jobs, one launch per transform (per HBM pass above 2^10)."""
     import torch
     engine.run_percall_dev(jobs)   # warm-up pass
@@ -565,7 +577,7 @@ def per_call(args, dist, ctx, stream, engine, jobs, batch, batched_value) -> dic
     e1.record(stream)
     torch.cuda.synchronize()
     ms = dist.max(e0.elapsed_time(e1) / reps)
-    v = batch.count * dist.world / (ms * 1e-3)
+    v = units / (ms * 1e-3)
     return {"value": v, "unit": UNIT, "ms_per_step": ms, "launches_per_step": launches // reps,
             "batched_over_per_call": batched_value / v}
 

@@ -157,6 +157,11 @@ _SIGS = [
                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     ("bntt_server_replay_ex", _I, [_P, ctypes.POINTER(RequestC), _S, _I, ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    ("bntt_split_by_cost", _I, [_P, _S, ctypes.c_uint32, _P]),
+    ("bntt_multi_create", _I, [ctypes.POINTER(_P), ctypes.POINTER(_P), _S]),
+    ("bntt_multi_destroy", _I, [_P]),
+    ("bntt_multi_split", _I, [_P, ctypes.POINTER(JobC), _S, _P]),
+    ("bntt_multi_run_host", _I, [_P, ctypes.POINTER(JobC), _S]),
     ("bntt_autotune", _I, [_P, ctypes.c_char_p]),
     ("bntt_autotune_load", _I, [_P, ctypes.c_char_p]),
     ("bntt_autotune_reset", _I, []),
@@ -449,6 +454,45 @@ class Batch:
     def close(self) -> None:
         if self._h:
             lib().bntt_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def split_by_cost(logns, parts: int) -> np.ndarray:
+    """bntt_split_by_cost: the owner (in [0, parts)) of each job of size
+    2^logns[i], longest first to the least-loaded part.  Needs no GPU."""
+    logns = np.ascontiguousarray(logns, dtype=np.uint32)
+    owner = np.empty(len(logns), dtype=np.uint32)
+    check(lib().bntt_split_by_cost(logns.ctypes.data, len(logns), parts, owner.ctypes.data))
+    return owner
+
+
+class Multi:
+    """One job list over several batches (one per device, own plans each):
+    split by cost, run from host buffers, no data exchanged between GPUs."""
+
+    def __init__(self, batches: list[Batch]):
+        self.batches = batches
+        arr = (ctypes.c_void_p * len(batches))(*[b.handle.value for b in batches])
+        self._h = ctypes.c_void_p()
+        check(lib().bntt_multi_create(ctypes.byref(self._h), arr, len(batches)))
+
+    def split(self, jobs) -> np.ndarray:
+        owner = np.empty(len(jobs), dtype=np.uint32)
+        check(lib().bntt_multi_split(self._h, jobs, len(jobs), owner.ctypes.data))
+        return owner
+
+    def run_host(self, jobs) -> None:
+        check(lib().bntt_multi_run_host(self._h, jobs, len(jobs)))
+
+    def close(self) -> None:
+        if self._h:
+            lib().bntt_multi_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

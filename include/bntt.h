@@ -298,6 +298,32 @@ int bntt_axpy_host(bntt_ctx *ctx, void *c, const void *a, const void *b, bntt_u1
 /* Kernel launches issued by this context since creation (all entry points). */
 uint64_t bntt_ctx_launch_count(bntt_ctx *ctx);
 
+/* ------------------------------------------------------------ several GPUs */
+/* The transforms of a job list are independent, so several devices share one
+ * list with no data exchange: the list is split by cost and each device runs
+ * its part on its own batch.  The reference has no multi-device path (one
+ * transform per call on one CPU core, src/ntt_scalar.c:582).
+ *
+ * bntt_split_by_cost: owner[i] in [0, parts) for each job of size 2^log2n[i]:
+ *   jobs in decreasing cost (N/2 * log2 N butterflies, ties by index), each to
+ *   the part with the least work so far (ties to the lower part).  Needs no
+ *   GPU; every caller splitting the same sizes gets the same owners.
+ * bntt_multi_create: one batch per device, each created on its own context
+ *   with its own plans (every device holds its own copy of the tables; no
+ *   device reads another's memory).  The batches must list plans of the same
+ *   sizes in the same order; a job's `plan` indexes that list.
+ * bntt_multi_split: bntt_split_by_cost over the job list's plan sizes.
+ * bntt_multi_run_host: splits the list, queues each part from host buffers on
+ *   its device (bntt_batch_run_host_async), then waits for all of them; the
+ *   outputs are in host memory when it returns.  BNTT_ETIMEOUT if a
+ *   device-side wait of any part gave up. */
+typedef struct bntt_multi bntt_multi;
+int bntt_split_by_cost(const uint32_t *log2n, size_t count, uint32_t parts, uint32_t *owner);
+int bntt_multi_create(bntt_multi **multi, bntt_batch *const *batches, size_t n);
+int bntt_multi_destroy(bntt_multi *multi);
+int bntt_multi_split(bntt_multi *multi, const bntt_job *jobs, size_t count, uint32_t *owner);
+int bntt_multi_run_host(bntt_multi *multi, const bntt_job *jobs, size_t count);
+
 /* ---------------------------------------------------------------- serving */
 /* A request loop with continuous batching.  Requests (forward NTTs of any
  * plan size, vvmul, axpy) name device-resident operands; the server admits
