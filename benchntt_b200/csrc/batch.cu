@@ -155,15 +155,8 @@ static const std::vector<int>& split_of(int n) {
   return table[n];
 }
 
-int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count,
-                   bool inverse) {
-  sc.djobs.resize(count);
-  sc.job_log2n.resize(count);
-  sc.large.clear();
-  sc.items.clear();
-  sc.pass_tiles.clear();
-  sc.nslots = 0;
-  // the plans' fields, looked up once instead of per job
+// The plans' fields, looked up once instead of per job.
+static void plan_fields(const bntt_batch* b, Schedule& sc, bool inverse) {
   const size_t np = b->plans.size();
   sc.plan_tw.resize(np);
   sc.plan_log2n.resize(np);
@@ -171,50 +164,32 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
     sc.plan_tw[k] = static_cast<const uint4*>(inverse ? b->plans[k]->tw_inv : b->plans[k]->tw);
     sc.plan_log2n[k] = (uint8_t)b->plans[k]->log2n;
   }
-  // one pass over the jobs: descriptors, sizes, small jobs counted per size
-  uint32_t per_size[11] = {};
-  const uint4* const* tw = sc.plan_tw.data();
-  const uint8_t* plog = sc.plan_log2n.data();
-  for (size_t i = 0; i < count; ++i) {
-    const bntt_job& jb = jobs[i];
-    BNTT_REQUIRE(jb.plan < np, "job %zu: plan index %u out of range", i, jb.plan);
-    BNTT_REQUIRE(jb.x && jb.y, "job %zu: NULL buffer", i);
-    BNTT_REQUIRE((((uintptr_t)jb.x | (uintptr_t)jb.y) & 15) == 0, "job %zu: buffers must be 16-byte aligned", i);
-    const uint32_t n = plog[jb.plan];
-    DevJob& d = sc.djobs[i];
-    d.x = static_cast<const uint4*>(jb.x);
-    d.y = static_cast<uint4*>(jb.y);
-    d.tw = tw[jb.plan];
-    d.log2n = n;
-    sc.job_log2n[i] = (uint8_t)n;
-    if (n <= 10) {
-      d.slot = 0;
-      ++per_size[n];
-    } else {
-      d.slot = (uint32_t)sc.nslots++;
-      sc.large.push_back((uint32_t)i);
-    }
-  }
-  // small jobs in size order, largest size first (a counting sort over the
-  // compact size array)
-  uint32_t first[11] = {}, fill[11];
+}
+
+// First position of each small size in the size-sorted order, largest size
+// first; returns the number of small jobs.
+static uint32_t size_offsets(const uint32_t per_size[11], uint32_t first[11]) {
   uint32_t small = 0;
+  first[0] = 0;
   for (int n = 10; n >= 1; --n) {
     first[n] = small;
     small += per_size[n];
   }
-  std::copy(first, first + 11, fill);
-  sc.order.resize(small);
-  const uint8_t* sizes = sc.job_log2n.data();
-  for (size_t i = 0; i < count; ++i) {
-    const uint32_t n = sizes[i];
-    if (n <= 10) sc.order[fill[n]++] = (uint32_t)i;
-  }
+  return small;
+}
+
+// The work items of a job list from its per-size counts and its large jobs
+// (sc.large / sc.large_n, slot = position there): passes that run first,
+// small tiles from the largest size down, the other passes in run order.
+static int make_items(const bntt_batch* b, Schedule& sc, const uint32_t per_size[11],
+                      const uint32_t first[11], bool inverse) {
+  sc.items.clear();
   for (auto& l : sc.later) l.clear();
+  sc.nslots = sc.large.size();
   sc.pass_tiles.assign(sc.nslots * kMaxPasses, 0);
-  for (const uint32_t ji : sc.large) {
-    const DevJob& d = sc.djobs[ji];
-    const int n = (int)d.log2n;
+  for (size_t slot = 0; slot < sc.large.size(); ++slot) {
+    const uint32_t ji = sc.large[slot];
+    const int n = sc.large_n[slot];
     const std::vector<int>& passes = split_of(n);
     BNTT_REQUIRE(!passes.empty() && passes.size() <= (size_t)kMaxPasses, "log2n %d needs too many passes", n);
     int s0 = 0;
@@ -226,7 +201,7 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
       const uint32_t tpc = (uint32_t)kShapes[shape].tpc;
       const uint64_t nsub = 1ull << (n - m);
       const uint32_t tiles = (uint32_t)((nsub + tpc - 1) / tpc);
-      sc.pass_tiles[d.slot * kMaxPasses + p] = tiles;
+      sc.pass_tiles[slot * kMaxPasses + p] = tiles;
       // position in the run order: forward pass p runs p-th, the inverse runs
       // the passes last to first
       const size_t run = inverse ? passes.size() - 1 - p : p;
@@ -234,7 +209,7 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
       WorkItem w{};
       w.shape = (uint16_t)shape;
       w.kind = ITEM_PASS;
-      w.a = (uint32_t)ji;
+      w.a = ji;
       w.pass = (uint16_t)p;
       w.wait = (uint16_t)((run > 0 ? 1 : 0) | (run == 0 ? 2 : 0) | (s0 << 8));
       for (uint32_t t = 0; t < tiles; ++t) {
@@ -244,8 +219,6 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
       s0 += m;
     }
   }
-  // queue: passes that run first, small tiles (largest size first), the
-  // other passes in run order
   sc.items.insert(sc.items.end(), sc.later[0].begin(), sc.later[0].end());
   for (int n = 10; n >= 1; --n) {
     const uint32_t cnt = per_size[n];
@@ -266,6 +239,85 @@ int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size
   return BNTT_OK;
 }
 
+// One validating pass over the jobs: sizes counted per small size, large
+// jobs listed.  `fill` also writes the jobs' device descriptors.
+static int scan_jobs(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count,
+                     uint32_t per_size[11], bool fill) {
+  const size_t np = b->plans.size();
+  const uint4* const* tw = sc.plan_tw.data();
+  const uint8_t* plog = sc.plan_log2n.data();
+  sc.large.clear();
+  sc.large_n.clear();
+  if (fill) {
+    sc.djobs.resize(count);
+    sc.job_log2n.resize(count);
+  }
+  for (size_t i = 0; i < count; ++i) {
+    const bntt_job& jb = jobs[i];
+    BNTT_REQUIRE(jb.plan < np, "job %zu: plan index %u out of range", i, jb.plan);
+    BNTT_REQUIRE(jb.x && jb.y, "job %zu: NULL buffer", i);
+    BNTT_REQUIRE((((uintptr_t)jb.x | (uintptr_t)jb.y) & 15) == 0, "job %zu: buffers must be 16-byte aligned", i);
+    const uint32_t n = plog[jb.plan];
+    if (n <= 10) {
+      ++per_size[n];
+    } else {
+      sc.large.push_back((uint32_t)i);
+      sc.large_n.push_back((uint8_t)n);
+    }
+    if (fill) {
+      DevJob& d = sc.djobs[i];
+      d.x = static_cast<const uint4*>(jb.x);
+      d.y = static_cast<uint4*>(jb.y);
+      d.tw = tw[jb.plan];
+      d.log2n = n;
+      d.slot = n <= 10 ? 0u : (uint32_t)(sc.large.size() - 1);
+      sc.job_log2n[i] = (uint8_t)n;
+    }
+  }
+  return BNTT_OK;
+}
+
+int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count,
+                   bool inverse) {
+  sc.dev_build = false;
+  plan_fields(b, sc, inverse);
+  uint32_t per_size[11] = {}, first[11], fill[11];
+  if (int rc = scan_jobs(b, sc, jobs, count, per_size, true)) return rc;
+  // small jobs in size order, largest size first (a counting sort over the
+  // compact size array)
+  const uint32_t small = size_offsets(per_size, first);
+  std::copy(first, first + 11, fill);
+  sc.order.resize(small);
+  const uint8_t* sizes = sc.job_log2n.data();
+  for (size_t i = 0; i < count; ++i) {
+    const uint32_t n = sizes[i];
+    if (n <= 10) sc.order[fill[n]++] = (uint32_t)i;
+  }
+  return make_items(b, sc, per_size, first, inverse);
+}
+
+// The host half of a schedule whose job descriptors and size order the
+// device builds (k_build_jobs): validation, sizes, work items, the table of
+// large jobs and the plans' table.  The caller's job array is read again by
+// the upload that follows.
+int build_schedule_dev(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count,
+                       bool inverse) {
+  sc.dev_build = true;
+  plan_fields(b, sc, inverse);
+  uint32_t per_size[11] = {};
+  if (int rc = scan_jobs(b, sc, jobs, count, per_size, false)) return rc;
+  sc.small = size_offsets(per_size, sc.first);
+  sc.count = count;
+  sc.raw = jobs;
+  sc.djobs.clear();
+  sc.order.clear();
+  sc.plan_ref.resize(b->plans.size());
+  for (size_t k = 0; k < b->plans.size(); ++k) sc.plan_ref[k] = PlanRef{sc.plan_tw[k], sc.plan_log2n[k], 0u};
+  sc.large_ref.resize(sc.large.size());
+  for (size_t k = 0; k < sc.large.size(); ++k) sc.large_ref[k] = LargeRef{sc.large[k], (uint32_t)k};
+  return make_items(b, sc, per_size, sc.first, inverse);
+}
+
 // Graphs of earlier job lists; the caller has synchronized `sc.stream`.
 static void destroy_retired(Schedule& sc) {
   for (cudaGraphExec_t e : sc.retired) cudaGraphExecDestroy(e);
@@ -284,11 +336,33 @@ static void destroy_retired(Schedule& sc) {
 static int upload(bntt_batch* b, Schedule& sc, cudaStream_t stream, bool inverse = false,
                   bool sticky_err = false, cudaStream_t copy_stream = nullptr) {
   bntt_ctx* c = b->ctx;
-  const size_t jb = sc.djobs.size() * sizeof(DevJob), ob = sc.order.size() * 4,
-               ib = sc.items.size() * sizeof(WorkItem), cb = (kCtlHeader + sc.nslots * kMaxPasses) * 4,
+  const size_t ib = sc.items.size() * sizeof(WorkItem), cb = (kCtlHeader + sc.nslots * kMaxPasses) * 4,
                pb = sc.pass_tiles.size() * 4;
   auto r256 = [](size_t v) { return (v + 255) & ~(size_t)255; };
-  const size_t o_ob = r256(jb), o_ib = o_ob + r256(ob), o_pb = o_ib + r256(ib), total = o_pb + r256(pb);
+  // Host-built: [djobs][order][items][pass tiles], all copied.  Device-built:
+  // [the caller's jobs][plans][large jobs][items][pass tiles] copied, then
+  // [djobs][order][fill counters] written on the device by k_build_jobs.
+  size_t o_jb = 0, o_ob = 0, o_ib = 0, o_pb = 0, staged = 0, total = 0;
+  size_t o_raw = 0, o_plan = 0, o_large = 0, o_fill = 0;
+  if (!sc.dev_build) {
+    const size_t jb = sc.djobs.size() * sizeof(DevJob), ob = sc.order.size() * 4;
+    o_ob = r256(jb);
+    o_ib = o_ob + r256(ob);
+    o_pb = o_ib + r256(ib);
+    staged = total = o_pb + r256(pb);
+  } else {
+    const size_t rb = sc.count * sizeof(bntt_job), plb = sc.plan_ref.size() * sizeof(PlanRef),
+                 lb = sc.large_ref.size() * sizeof(LargeRef);
+    o_plan = r256(rb);
+    o_large = o_plan + r256(plb);
+    o_ib = o_large + r256(lb);
+    o_pb = o_ib + r256(ib);
+    staged = o_pb + r256(pb);
+    o_jb = staged;
+    o_ob = o_jb + r256(sc.count * sizeof(DevJob));
+    o_fill = o_ob + r256((size_t)sc.small * 4);
+    total = o_fill + 256;
+  }
   if (sc.exec) {
     sc.retired.push_back(sc.exec);
     sc.exec = nullptr;
@@ -306,16 +380,23 @@ static int upload(bntt_batch* b, Schedule& sc, cudaStream_t stream, bool inverse
   sc.stage_next ^= 1;
   if (sc.stage_done[si]) BNTT_CK(cudaEventSynchronize(sc.stage_done[si]));
   else BNTT_CK(cudaEventCreateWithFlags(&sc.stage_done[si], cudaEventDisableTiming));
-  if (sc.stage_cap[si] < total) {
+  if (sc.stage_cap[si] < staged) {
     if (sc.stage[si]) cudaFreeHost(sc.stage[si]);
     sc.stage[si] = nullptr;
     sc.stage_cap[si] = 0;
-    BNTT_CK(cudaMallocHost(&sc.stage[si], total + total / 2));
-    sc.stage_cap[si] = total + total / 2;
+    BNTT_CK(cudaMallocHost(&sc.stage[si], staged + staged / 2));
+    sc.stage_cap[si] = staged + staged / 2;
   }
   char* h = static_cast<char*>(sc.stage[si]);
-  if (jb) memcpy(h, sc.djobs.data(), jb);
-  if (ob) memcpy(h + o_ob, sc.order.data(), ob);
+  if (!sc.dev_build) {
+    if (!sc.djobs.empty()) memcpy(h + o_jb, sc.djobs.data(), sc.djobs.size() * sizeof(DevJob));
+    if (!sc.order.empty()) memcpy(h + o_ob, sc.order.data(), sc.order.size() * 4);
+  } else {
+    if (sc.count) memcpy(h + o_raw, sc.raw, sc.count * sizeof(bntt_job));
+    memcpy(h + o_plan, sc.plan_ref.data(), sc.plan_ref.size() * sizeof(PlanRef));
+    if (!sc.large_ref.empty()) memcpy(h + o_large, sc.large_ref.data(), sc.large_ref.size() * sizeof(LargeRef));
+    sc.raw = nullptr;  // the caller's array is not read after this point
+  }
   if (ib) memcpy(h + o_ib, sc.items.data(), ib);
   if (pb) {
     uint32_t* t = reinterpret_cast<uint32_t*>(h + o_pb);
@@ -324,7 +405,7 @@ static int upload(bntt_batch* b, Schedule& sc, cudaStream_t stream, bool inverse
       for (size_t i = 0; i < sc.pass_tiles.size(); ++i) t[i] += 1;
   }
   char* d = static_cast<char*>(sc.d_sched[set]);
-  BNTT_CK(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, cs));
+  BNTT_CK(cudaMemcpyAsync(d, h, staged, cudaMemcpyHostToDevice, cs));
   BNTT_CK(cudaEventRecord(sc.stage_done[si], cs));
   if (cs != stream) {
     if (!sc.set_ready) BNTT_CK(cudaEventCreateWithFlags(&sc.set_ready, cudaEventDisableTiming));
@@ -332,6 +413,18 @@ static int upload(bntt_batch* b, Schedule& sc, cudaStream_t stream, bool inverse
     BNTT_CK(cudaStreamWaitEvent(stream, sc.set_ready, 0));
   }
   sc.cur = set;
+  if (sc.dev_build && sc.count) {  // descriptors and size order, on the device, before the launches
+    BNTT_CK(cudaMemsetAsync(d + o_fill, 0, 256, stream));
+    if (int rc = launch_build_jobs(reinterpret_cast<const bntt_job*>(d + o_raw), sc.count,
+                                   reinterpret_cast<const PlanRef*>(d + o_plan),
+                                   reinterpret_cast<const LargeRef*>(d + o_large),
+                                   (uint32_t)sc.large_ref.size(), sc.first, reinterpret_cast<uint32_t*>(d + o_fill),
+                                   reinterpret_cast<DevJob*>(d + o_jb), reinterpret_cast<uint32_t*>(d + o_ob),
+                                   stream))
+      return rc;
+    c->launches++;
+    b->last_launches++;
+  }
   if (sticky_err) BNTT_CK(cudaMemsetAsync(sc.d_ctl, 0, cb, stream));
   sc.stream = stream;
   sc.inverse = inverse;
@@ -351,7 +444,7 @@ static int upload(bntt_batch* b, Schedule& sc, cudaStream_t stream, bool inverse
   BatchArgs& ba = sc.args;
   ba.items = reinterpret_cast<const WorkItem*>(d + o_ib);
   ba.nitems = (uint32_t)sc.items.size();
-  ba.jobs = reinterpret_cast<const DevJob*>(d);
+  ba.jobs = reinterpret_cast<const DevJob*>(d + o_jb);
   ba.order = reinterpret_cast<const uint32_t*>(d + o_ob);
   ba.ctl = static_cast<uint32_t*>(sc.d_ctl);
   ba.pass_tiles = reinterpret_cast<const uint32_t*>(d + o_pb);
@@ -488,7 +581,7 @@ int bntt_batch_run_dev(bntt_batch* b, const bntt_job* jobs, size_t count) {
                     memcmp(b->last_jobs.data(), jobs, count * sizeof(bntt_job)) == 0;
   if (!same) {  // a new list is launched directly; a graph is captured if it comes again
     b->last_jobs.clear();
-    if (int rc = build_schedule(b, b->main, jobs, count)) return rc;
+    if (int rc = build_schedule_dev(b, b->main, jobs, count, false)) return rc;
     if (int rc = upload(b, b->main, b->ctx->stream, false, false, b->upload_stream)) return rc;
     if (!inject) b->last_jobs.assign(jobs, jobs + count);
   } else if (int rc = capture(b, b->main)) {
@@ -514,7 +607,7 @@ int bntt_batch_run_inverse_dev(bntt_batch* b, const bntt_job* jobs, size_t count
                     memcmp(b->inv_last_jobs.data(), jobs, count * sizeof(bntt_job)) == 0;
   if (!same) {
     b->inv_last_jobs.clear();
-    if (int rc = build_schedule(b, b->inv, jobs, count, true)) return rc;
+    if (int rc = build_schedule_dev(b, b->inv, jobs, count, true)) return rc;
     if (int rc = upload(b, b->inv, b->ctx->stream, true, false, b->upload_stream)) return rc;
     b->inv_last_jobs.assign(jobs, jobs + count);
   } else if (int rc = capture(b, b->inv)) {

@@ -41,6 +41,22 @@ struct DevJob {
   uint32_t slot;  // counter slot for large jobs
 };
 
+// Device build of a new job list's descriptors (k_build_jobs): a plan's table
+// and size, and a large job's counter slot.
+struct PlanRef {
+  const uint4* tw;
+  uint32_t log2n;
+  uint32_t pad;
+};
+struct LargeRef {
+  uint32_t job;
+  uint32_t slot;
+};
+// first position of each small size in the size-sorted order
+struct SizeFirst {
+  uint32_t first[11];
+};
+
 enum : uint32_t { ITEM_SMALL = 0, ITEM_PASS = 1 };
 
 struct WorkItem {

@@ -21,9 +21,21 @@ struct Schedule {
   std::vector<WorkItem> later[kMaxPasses];  // build scratch: pass items by run position
   std::vector<uint8_t> job_log2n;           // build scratch: each job's size
   std::vector<uint32_t> large;              // build scratch: jobs above 2^10 points
+  std::vector<uint8_t> large_n;             // build scratch: their sizes
   std::vector<const uint4*> plan_tw;        // build scratch: the plans' tables
   std::vector<uint8_t> plan_log2n;
   size_t nslots = 0;
+  // device-built schedules (bntt_batch_run_dev / run_inverse_dev): djobs and
+  // order are left empty on the host; k_build_jobs writes them on the device
+  // from a copy of the caller's job array, the plans' table and the large
+  // jobs' slots
+  bool dev_build = false;
+  size_t count = 0;                         // jobs in the list
+  uint32_t small = 0;                       // jobs of at most 2^10 points
+  uint32_t first[11] = {};                  // first position of each small size
+  const bntt_job* raw = nullptr;            // the caller's jobs (valid during the upload)
+  std::vector<PlanRef> plan_ref;
+  std::vector<LargeRef> large_ref;
   // device copies of djobs, order, items and pass_tiles in one buffer, two
   // buffers used in turn: a new job list is copied into the one the running
   // launches do not read, so the copy overlaps them
@@ -102,4 +114,14 @@ size_t shape_smem(int s);
 // passes of a large job queued last to first)
 int build_schedule(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count,
                    bool inverse = false);
+// The host half of a schedule whose descriptors and size order k_build_jobs
+// writes on the device; the job array must stay valid until the upload.
+int build_schedule_dev(const bntt_batch* b, Schedule& sc, const bntt_job* jobs, size_t count,
+                       bool inverse = false);
+// k_build_jobs (batch_build.cu): descriptors of `count` jobs and the order of
+// the small ones, from device copies of the job array, the plans' table and
+// the large jobs' slots; fill[11] must be zero.
+int launch_build_jobs(const bntt_job* raw, size_t count, const PlanRef* plans, const LargeRef* large,
+                      uint32_t nlarge, const uint32_t first[11], uint32_t* fill, DevJob* djobs,
+                      uint32_t* order, cudaStream_t stream);
 }  // namespace bntt

@@ -67,6 +67,14 @@ def test_mixed_small_sizes(ctx):
     s = Setup(ctx, b)
     s.engine.run_dev(s.jobs())
     assert s.engine.status() == bn.OK
+    # a new job list: the device-side schedule build, then the persistent kernel
+    assert s.engine.last_launches == 2
+    assert np.array_equal(s.output(), s.expected())
+    # the same list again: one graph replay of the persistent kernel
+    zero = np.zeros((b.total, 2), dtype=np.uint64)
+    bn.check(bn.lib().bntt_copy_h2d(ctx.handle, s.dy.ptr, zero.ctypes.data, zero.nbytes))
+    s.engine.run_dev(s.jobs())
+    assert s.engine.status() == bn.OK
     assert s.engine.last_launches == 1
     assert np.array_equal(s.output(), s.expected())
     s.close()
@@ -312,7 +320,7 @@ def test_forward_then_inverse_batch_round_trip(ctx):
     s.engine.run_inverse_dev(back)
     assert s.engine.status() == bn.OK
     assert np.array_equal(zs.to_array(), s.x)
-    assert s.engine.last_launches == 1
+    assert s.engine.last_launches == 2   # schedule build on the device, then the persistent kernel
     zs.free()
     s.close()
 
