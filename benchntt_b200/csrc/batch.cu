@@ -599,7 +599,7 @@ int bntt_batch_run_inverse_dev(bntt_batch* b, const bntt_job* jobs, size_t count
   b->last_launches = 0;
   b->noalloc_err = nullptr;
   if (count == 0) return BNTT_OK;
-  BNTT_REQUIRE(b->fast, "the inverse transform needs q = 2^124 - k (k < 2^31), mu = floor(2^251/q) "
+  BNTT_REQUIRE(b->fast, "the inverse transform needs q = 2^124 - k (k < 2^28), mu = floor(2^251/q) "
                "and the default arithmetic");
   for (bntt_plan* p : b->plans)
     if (int rc = plan_ensure_inverse(p)) return rc;

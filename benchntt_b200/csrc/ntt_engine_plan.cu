@@ -14,7 +14,7 @@
 //
 // Sums here are exact mod q (no reference quirk applies: the reference has
 // no such code); results are canonical residues in [0, q).  The fast
-// pseudo-Mersenne multiply is required (q = 2^124 - k, k < 2^31).
+// pseudo-Mersenne multiply is required (q = 2^124 - k, k < 2^28).
 //
 // Kernels: the runtime-size tile engine (ntt_engine.cuh) in inverse mode,
 // one launch per HBM pass in reverse pass order (the pass over the low index
@@ -217,7 +217,7 @@ int inverse_on(bntt_plan* p, void* x, const void* y, size_t batch, cudaStream_t 
 }  // namespace
 
 int plan_ensure_inverse(bntt_plan* p) {
-  if (!p->fast) return set_error(BNTT_EINVAL, "the inverse transform needs q = 2^124 - k (k < 2^31), mu = floor(2^251/q)");
+  if (!p->fast) return set_error(BNTT_EINVAL, "the inverse transform needs q = 2^124 - k (k < 2^28), mu = floor(2^251/q)");
   return ensure_inverse(p);
 }
 
@@ -242,7 +242,7 @@ extern "C" int bntt_ntt_inverse_dev(bntt_plan* p, void* x, const void* y, size_t
   BNTT_REQUIRE(x && y, "NULL buffer");
   BNTT_REQUIRE(((uintptr_t)x & 15) == 0 && ((uintptr_t)y & 15) == 0,
                "device buffers must be 16-byte aligned");
-  BNTT_REQUIRE(p->fast, "the inverse transform needs q = 2^124 - k (k < 2^31), mu = floor(2^251/q)");
+  BNTT_REQUIRE(p->fast, "the inverse transform needs q = 2^124 - k (k < 2^28), mu = floor(2^251/q)");
   if (int rc = ctx_use_device(p->ctx)) return rc;
   if (int rc = ensure_inverse(p)) return rc;
   return inverse_on(p, x, y, batch, p->ctx->stream);

@@ -22,7 +22,7 @@
 // Host arithmetic here is exact for every q in (2^123, 2^124): a 256-bit
 // product and a Barrett quotient that is at most one short, then a
 // correction.  Device tables use the pseudo-Mersenne multiply, which is exact
-// for the moduli this mode produces (k < 2^31).
+// for the moduli this mode produces (k < 2^28).
 #include <algorithm>
 #include <vector>
 
@@ -149,7 +149,7 @@ int bntt_ntt_prime(unsigned log2_order, bntt_modulus* m) {
   const u128 top = (u128)1 << 124;
   for (uint64_t c = 1;; ++c) {
     const u128 k = ((u128)c << log2_order) - 1;
-    if (k >= ((u128)1 << 31)) break;
+    if (k >= ((u128)1 << 28)) break;
     const u128 q = top - k;
     const u128 mu = barrett_mu(q);
     if (miller_rabin(q, mu)) {
@@ -158,7 +158,7 @@ int bntt_ntt_prime(unsigned log2_order, bntt_modulus* m) {
       return BNTT_OK;
     }
   }
-  return set_error(BNTT_EINVAL, "no prime 2^124 - (c*2^%u - 1) with c*2^%u - 1 < 2^31", log2_order,
+  return set_error(BNTT_EINVAL, "no prime 2^124 - (c*2^%u - 1) with c*2^%u - 1 < 2^28", log2_order,
                    log2_order);
 }
 
@@ -219,7 +219,7 @@ int bntt_plan_create_negacyclic(bntt_ctx* c, bntt_plan** out, unsigned log2n, co
   BNTT_REQUIRE(m, "NULL argument");
   const u128 q = to_u128(m->q), mu = to_u128(m->mu), p = to_u128(psi);
   BNTT_REQUIRE(modulus_fast(q, mu, nullptr),
-               "root-power tables are built on the device for q = 2^124 - k (k < 2^31), "
+               "root-power tables are built on the device for q = 2^124 - k (k < 2^28), "
                "mu = floor(2^251/q); build others with bntt_twiddles_negacyclic");
   BNTT_REQUIRE(log2n >= 1 && log2n <= 24, "log2n %u outside [1, 24]", log2n);
   BNTT_REQUIRE(p < q && host_powmod(p, (u128)1 << log2n, q, mu) == q - 1,

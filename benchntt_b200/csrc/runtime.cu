@@ -47,17 +47,19 @@ u128 barrett_mu(u128 q) {
 }
 
 // The pseudo-Mersenne multiply equals the reference mulmod128 when
-//   2^123 < q = 2^124 - k,  1 <= k < 2^31,  mu = floor(2^251 / q):
+//   2^123 < q = 2^124 - k,  1 <= k < 2^28,  mu = floor(2^251 / q):
 // for operands below 2^124 the reference's intermediate sums cannot wrap
 // (mu = 2^127 + d with d < 2^35, so its mulhi128 cross terms stay below
 // 2^128), and its quotient estimate is floor(P/q) or one less (the two
 // truncations lose less than 2^122/q + P/2^251 < 1/2 + 1/8), so one
-// conditional subtraction returns P mod q.
+// conditional subtraction returns P mod q.  (The reference's exactness holds
+// up to k < 2^31; the device multiply folds at 2^128 with the factor 16k,
+// which must fit in 32 bits.)
 bool modulus_fast(u128 q, u128 mu, uint32_t* k_out) {
   const u128 top = (u128)1 << 124;
   if (q >= top || q <= ((u128)1 << 123)) return false;
   const u128 k = top - q;
-  if (k >= ((u128)1 << 31)) return false;
+  if (k >= ((u128)1 << 28)) return false;
   if (mu != barrett_mu(q)) return false;
   if (k_out) *k_out = (uint32_t)k;
   return true;

@@ -9,13 +9,14 @@
 //
 // Two multiply policies produce results bit-identical to the reference
 // mulmod128 (src/ntt_scalar.c:173-199):
-//   ArithFast -- q = 2^124 - k with k < 2^31 and mu = floor(2^251 / q) (both
+//   ArithFast -- q = 2^124 - k with k < 2^28 and mu = floor(2^251 / q) (both
 //     reference primes and the NTT-friendly primes of roots.cu).  For such (q, mu) and operands below 2^124 the
 //     reference's Barrett quotient is within one of the true quotient, so its
 //     single conditional subtraction always lands in [0, q): the reference
 //     returns exactly a*b mod q.  ArithFast computes that value with a
-//     pseudo-Mersenne fold (2^124 == k mod q): 16 limb products for a*b, 4 for
-//     the first fold, 2 for the second, one conditional subtraction.
+//     pseudo-Mersenne fold (2^128 == 16k, 2^124 == k mod q): 16 limb products
+//     for a*b, 4 for the first fold, 1 for the second, one conditional
+//     subtraction.
 //   ArithRef  -- every other (q, mu): a replica of the reference's 64-bit word
 //     data flow, including the points where it drops carries, so it matches
 //     for arbitrary 128-bit inputs.
@@ -217,44 +218,41 @@ __device__ __forceinline__ void mul_128x128(const U128& a, const U128& b, uint32
         "r"(b.w[2]), "r"(b.w[3]));
 }
 
-// r = P mod q for q = 2^124 - k, P < 2^248, k < 2^31.
-//   P = H*2^124 + L      ->  t = L + H*k            (< 2^155 + 2^124)
-//   t = H2*2^124 + L2    ->  r = L2 + H2*k          (H2 <= 2^31, so r < 2^124 + 2^62 < 2q)
-//   r >= q ? r - q : r, tested as bit 124 of r + k.
-// The reference moduli (k = 719, 59) and the NTT-friendly primes
-// 2^124 - (c*2^t - 1) all satisfy k < 2^31.
+// r = P mod q for q = 2^124 - k, P < 2^248, k < 2^28, folding first at the
+// limb boundary 2^128 (2^128 = 16 * 2^124 == 16k mod q), which needs no
+// shifts of P:
+//   P = H*2^128 + L      ->  t = L + H*16k          (< 2^128 + 2^152: 5 limbs)
+//   t = h*2^124 + l      ->  r = l + h*k            (h < 2^29; r < 2^124 + 2^57 < 2q)
+//   r >= q ? r - q : r, tested as bit 124 of r + k; r >= q needs r's top
+//   limb at least 0x0FFFFFFF, about one case in 2^28 for spread residues, so
+//   the exact test and the subtraction sit behind a branch.
+// Folding at 2^124 twice instead costs six more ALU instructions (funnel
+// shifts of P, the second fold's product added outside the multiply-add
+// chain): 204 against 209 G butterflies/s in the register-only probe.  Both reference
+// moduli and every prime bntt_ntt_prime returns have k < 2^28.
 __device__ __forceinline__ U128 reduce_pm124(const uint32_t p[8], uint32_t k) {
-  const uint32_t h0 = __funnelshift_r(p[3], p[4], 28);
-  const uint32_t h1 = __funnelshift_r(p[4], p[5], 28);
-  const uint32_t h2 = __funnelshift_r(p[5], p[6], 28);
-  const uint32_t h3 = __funnelshift_r(p[6], p[7], 28);
-  const uint32_t l3 = p[3] & 0x0FFFFFFFu;
+  const uint32_t c = k << 4;
   uint32_t t0, t1, t2, t3, t4;
   asm("mad.lo.cc.u32  %0, %5, %9, %10;\n\t"
       "madc.lo.cc.u32 %1, %6, %9, %11;\n\t"
       "madc.lo.cc.u32 %2, %7, %9, %12;\n\t"
       "madc.lo.cc.u32 %3, %8, %9, %13;\n\t"
-      "addc.u32       %4, 0, 0;\n\t"
+      "madc.hi.u32    %4, %8, %9, 0;\n\t"
       "mad.hi.cc.u32  %1, %5, %9, %1;\n\t"
       "madc.hi.cc.u32 %2, %6, %9, %2;\n\t"
       "madc.hi.cc.u32 %3, %7, %9, %3;\n\t"
-      "madc.hi.u32    %4, %8, %9, %4;\n\t"
+      "addc.u32       %4, %4, 0;\n\t"
       : "=&r"(t0), "=&r"(t1), "=&r"(t2), "=&r"(t3), "=&r"(t4)
-      : "r"(h0), "r"(h1), "r"(h2), "r"(h3), "r"(k), "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(l3));
-  const uint32_t h2w = __funnelshift_r(t3, t4, 28);  // t >> 124 (t < 2^156)
+      : "r"(p[4]), "r"(p[5]), "r"(p[6]), "r"(p[7]), "r"(c), "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(p[3]));
+  const uint32_t h = __funnelshift_r(t3, t4, 28);  // t >> 124
   U128 r;
-  asm("mul.lo.u32     %3, %8, %9;\n\t"
-      "add.cc.u32     %0, %4, %3;\n\t"
-      "mul.hi.u32     %3, %8, %9;\n\t"
-      "addc.cc.u32    %1, %5, %3;\n\t"
-      "addc.cc.u32    %2, %6, 0;\n\t"
-      "addc.u32       %3, %7, 0;\n\t"
-      : "=&r"(r.w[0]), "=&r"(r.w[1]), "=&r"(r.w[2]), "=&r"(r.w[3])
-      : "r"(t0), "r"(t1), "r"(t2), "r"(t3 & 0x0FFFFFFFu), "r"(h2w), "r"(k));
-  // r < 2^124 + 2^62 < 2q.  r >= q needs r's top limb >= q's (0x0FFFFFFF
-  // for every k < 2^96): for residues spread over [0, q) that is about one
-  // case in 2^28, so the exact test and subtraction sit behind a branch.
-  if (__builtin_expect(r.w[3] >= 0x0FFFFFFFu, 0)) {
+  asm("mad.lo.cc.u32  %0, %4, %5, %6;\n\t"
+      "madc.hi.cc.u32 %1, %4, %5, %7;\n\t"
+      "addc.cc.u32    %2, %8, 0;\n\t"
+      "addc.u32       %3, %9, 0;\n\t"
+      : "=r"(r.w[0]), "=r"(r.w[1]), "=r"(r.w[2]), "=r"(r.w[3])
+      : "r"(h), "r"(k), "r"(t0), "r"(t1), "r"(t2), "r"(t3 & 0x0FFFFFFFu));
+  if (__builtin_expect(r.w[3] >= 0x0FFFFFFFu, 0)) {  // r >= q is possible only here
     uint32_t s0, s1, s2, s3;
     asm("add.cc.u32  %0, %4, %8;\n\t"
         "addc.cc.u32 %1, %5, 0;\n\t"
@@ -262,7 +260,7 @@ __device__ __forceinline__ U128 reduce_pm124(const uint32_t p[8], uint32_t k) {
         "addc.u32    %3, %7, 0;\n\t"
         : "=r"(s0), "=r"(s1), "=r"(s2), "=r"(s3)
         : "r"(r.w[0]), "r"(r.w[1]), "r"(r.w[2]), "r"(r.w[3]), "r"(k));
-    if (s3 >> 28) {  // r + k >= 2^124, i.e. r >= q: r - q = r + k - 2^124
+    if (s3 >> 28) {  // r + k >= 2^124, i.e. r >= q
       r.w[0] = s0; r.w[1] = s1; r.w[2] = s2; r.w[3] = s3 & 0x0FFFFFFFu;
     }
   }

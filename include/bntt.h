@@ -66,7 +66,7 @@ typedef struct bntt_modulus {
 #define BNTT_LAYOUT_U128 1
 
 /* Arithmetic selection.
- * AUTO: a pseudo-Mersenne multiply when q = 2^124 - k (k < 2^31) and
+ * AUTO: a pseudo-Mersenne multiply when q = 2^124 - k (k < 2^28) and
  *       mu = floor(2^251/q) -- both reference moduli and the NTT-friendly
  *       primes of bntt_ntt_prime -- for which the
  *       reference's Barrett reduction provably returns a*b mod q exactly;
@@ -147,7 +147,7 @@ unsigned bntt_plan_log2n(const bntt_plan *plan);
  *
  * bntt_ntt_prime: q = 2^124 - (c*2^log2_order - 1) for the smallest c >= 1
  *   that passes a Miller-Rabin test to the first 24 prime bases, with
- *   mu = floor(2^251/q); k = 2^124 - q < 2^31, so the default fast multiply
+ *   mu = floor(2^251/q); k = 2^124 - q < 2^28, so the default fast multiply
  *   applies.  EINVAL if no such prime exists.
  * bntt_root_of_unity: a primitive 2^log2_order-th root of unity mod q
  *   (g^((q-1)/2^log2_order) for the smallest g >= 2 of that exact order).
@@ -177,7 +177,7 @@ int bntt_ntt_forward_host(bntt_plan *plan, void *y, const void *x, size_t batch)
  * N^-1, so ntt^-1(ntt(x)) = x for every table whose entries are invertible
  * mod a prime q.  With a negacyclic plan it is the inverse negacyclic NTT.
  * Results are canonical residues in [0, q).  Needs the fast multiply
- * (q = 2^124 - k, k < 2^31, mu = floor(2^251/q)); the inverse table is
+ * (q = 2^124 - k, k < 2^28, mu = floor(2^251/q)); the inverse table is
  * built on the first call (EINVAL if a twiddle is 0 mod q or q is not
  * prime). */
 int bntt_ntt_inverse_dev(bntt_plan *plan, void *x, const void *y, size_t batch);

@@ -317,11 +317,11 @@ def is_probable_prime(n: int) -> bool:
 
 
 def ntt_prime_py(log2_order: int) -> int:
-    """Smallest-c prime 2^124 - (c*2^log2_order - 1) with k < 2^31."""
+    """Smallest-c prime 2^124 - (c*2^log2_order - 1) with k < 2^28."""
     c = 1
     while True:
         k = (c << log2_order) - 1
-        assert k < 1 << 31, "no prime in range"
+        assert k < 1 << 28, "no prime in range"
         if is_probable_prime((1 << 124) - k):
             return (1 << 124) - k
         c += 1

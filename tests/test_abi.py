@@ -74,8 +74,8 @@ def test_status_strings_and_reference_moduli():
 
 
 @pytest.mark.parametrize("q,fast", [(C.Q_NTT, 1), (C.Q_BLAS, 1), ((1 << 124) - 3, 1),
-                                    ((1 << 124) - (1 << 14), 1), ((1 << 124) - (1 << 31) + 1, 1),
-                                    ((1 << 124) - (1 << 31), 0), ((1 << 123) + 5, 0),
+                                    ((1 << 124) - (1 << 14), 1), ((1 << 124) - (1 << 28) + 1, 1),
+                                    ((1 << 124) - (1 << 28), 0), ((1 << 124) - (1 << 31) + 1, 0), ((1 << 123) + 5, 0),
                                     ((1 << 127) + 99, 0)])
 def test_fast_path_eligibility(q, fast):
     mu = ((1 << 251) // q) & ((1 << 128) - 1)

@@ -31,7 +31,7 @@ def test_prime_search_matches_python(t):
     q, mu = bn.ntt_prime(t)
     assert q == C.ntt_prime_py(t)
     assert mu == (1 << 251) // q
-    assert (q - 1) % (1 << t) == 0 and (1 << 124) - q < 1 << 31
+    assert (q - 1) % (1 << t) == 0 and (1 << 124) - q < 1 << 28
     assert bn.lib().bntt_modulus_is_fast(ctypes.byref(bn.modulus(q, mu))) == 1
 
 
@@ -156,9 +156,9 @@ def test_reference_live_with_friendly_prime(logn):
 
 
 def test_fast_multiply_bound_widened():
-    """The pseudo-Mersenne path covers k < 2^31 (both reference moduli and
-    every prime of this mode); k = 2^31 and a wrong mu fall back."""
-    for k, fast in ((719, 1), (59, 1), ((1 << 31) - 1, 1), (1 << 31, 0)):
+    """The pseudo-Mersenne path covers k < 2^28 (both reference moduli and
+    every prime of this mode); k = 2^28 and a wrong mu fall back."""
+    for k, fast in ((719, 1), (59, 1), ((1 << 28) - 1, 1), (1 << 28, 0), ((1 << 31) - 1, 0)):
         q = (1 << 124) - k
         assert bn.lib().bntt_modulus_is_fast(ctypes.byref(bn.modulus(q))) == fast
     q = (1 << 124) - 0x7bfffff
