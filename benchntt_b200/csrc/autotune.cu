@@ -2,8 +2,10 @@
 //
 // For every size the library has several compiled shapes: elements per thread
 // (radix 8 or 16 register tiles, which also sets the number of shared-memory
-// passes), transforms per CTA (CTA shape), and register budgets (two or three
-// resident CTAs per SM).  The tuner times each candidate on this device with
+// passes), transforms per CTA (CTA shape), register budgets (two or three
+// resident CTAs per SM), inputs read from HBM by the first pass or staged
+// into shared memory a tile ahead, and the twiddle table read through L1 or
+// copied into shared memory per CTA (twiddle placement).  The tuner times each candidate on this device with
 // seeded data larger than L2 and makes the fastest the default for plans and
 // batches created afterwards in the process.  Choices can be written to and
 // read from a small text file (keyed by device name and SM count).
@@ -135,8 +137,8 @@ int bntt_autotune(bntt_ctx* c, const char* path) {
           float ms = 0;
           if ((rc = time_sub(c, &k, g, mp, 5, &ms)) != 0) break;
           char line[160];
-          snprintf(line, sizeof(line), "# sub m=%d map=%d fast=%d logr=%d tpc=%d minb=%d %.4f ms\n", m,
-                   map, fast, k.logr, k.tpc, k.minb, ms);
+          snprintf(line, sizeof(line), "# sub m=%d map=%d fast=%d logr=%d tpc=%d minb=%d src=%d %.4f ms\n",
+                   m, map, fast, k.logr, k.tpc, k.minb, k.src, ms);
           report += line;
           if (ms < best_ms) {
             best_ms = ms;
@@ -147,8 +149,8 @@ int bntt_autotune(bntt_ctx* c, const char* path) {
           std::lock_guard<std::mutex> g(g_tune_mu);
           g_sub_choice[m][map][fast] = best;
           char line[128];
-          snprintf(line, sizeof(line), "sub %d %d %d %d %d %d\n", m, map, fast, best->logr, best->tpc,
-                   best->minb);
+          snprintf(line, sizeof(line), "sub %d %d %d %d %d %d %d\n", m, map, fast, best->logr, best->tpc,
+                   best->minb, best->src);
           report += line;
         }
       }
@@ -217,10 +219,12 @@ int bntt_autotune_load(bntt_ctx* c, const char* path) {
       rc = set_error(BNTT_EINVAL, "%s was tuned for another device (%s)", path, head.c_str());
   }
   while (!rc && fgets(line, sizeof(line), f)) {
-    int m, map, fast, logr, tpc, minb;
-    if (sscanf(line, "sub %d %d %d %d %d %d", &m, &map, &fast, &logr, &tpc, &minb) == 6) {
+    int m, map, fast, logr, tpc, minb, src = 0;
+    const int got = sscanf(line, "sub %d %d %d %d %d %d %d", &m, &map, &fast, &logr, &tpc, &minb, &src);
+    if (got == 6 || got == 7) {  // files without the last field name an unstaged shape
       for (const SubKernel& k : sub_kernels())
-        if (k.m == m && k.map == map && k.fast == fast && k.logr == logr && k.tpc == tpc && k.minb == minb) {
+        if (k.m == m && k.map == map && k.fast == fast && k.logr == logr && k.tpc == tpc && k.minb == minb &&
+            k.src == src) {
           std::lock_guard<std::mutex> g(g_tune_mu);
           g_sub_choice[m][map][fast] = &k;
         }

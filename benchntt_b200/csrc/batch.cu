@@ -93,6 +93,8 @@ void free_schedule(bntt_ctx* c, Schedule& s) {
     if (s.stage_done[i]) cudaEventSynchronize(s.stage_done[i]);
     if (s.set_free[i]) cudaEventSynchronize(s.set_free[i]);
     if (s.stage[i]) cudaFreeHost(s.stage[i]);
+    s.staged_raw = nullptr;
+    s.staged_count = 0;
     if (s.stage_done[i]) cudaEventDestroy(s.stage_done[i]);
     if (s.set_free[i]) cudaEventDestroy(s.set_free[i]);
     if (s.d_sched[i]) ctx_free(c, s.d_sched[i]);
@@ -393,6 +395,8 @@ static int upload(bntt_batch* b, Schedule& sc, cudaStream_t stream, bool inverse
     if (!sc.order.empty()) memcpy(h + o_ob, sc.order.data(), sc.order.size() * 4);
   } else {
     if (sc.count) memcpy(h + o_raw, sc.raw, sc.count * sizeof(bntt_job));
+    sc.staged_raw = reinterpret_cast<const bntt_job*>(h + o_raw);
+    sc.staged_count = sc.count;
     memcpy(h + o_plan, sc.plan_ref.data(), sc.plan_ref.size() * sizeof(PlanRef));
     if (!sc.large_ref.empty()) memcpy(h + o_large, sc.large_ref.data(), sc.large_ref.size() * sizeof(LargeRef));
     sc.raw = nullptr;  // the caller's array is not read after this point
@@ -570,6 +574,12 @@ int bntt_batch_destroy(bntt_batch* b) {
   return BNTT_OK;
 }
 
+// The job list `sc` was last uploaded with (its staged copy), on `stream`.
+static bool same_list(const Schedule& sc, const bntt_job* jobs, size_t count, cudaStream_t stream) {
+  return sc.staged_raw && sc.staged_count == count && sc.stream == stream &&
+         memcmp(sc.staged_raw, jobs, count * sizeof(bntt_job)) == 0;
+}
+
 int bntt_batch_run_dev(bntt_batch* b, const bntt_job* jobs, size_t count) {
   BNTT_REQUIRE(b && (jobs || count == 0), "NULL argument");
   if (int rc = ctx_use_device(b->ctx)) return rc;
@@ -577,13 +587,12 @@ int bntt_batch_run_dev(bntt_batch* b, const bntt_job* jobs, size_t count) {
   b->noalloc_err = nullptr;
   if (count == 0) return BNTT_OK;
   const bool inject = b->inject_polls != 0;
-  const bool same = !inject && b->last_jobs.size() == count && b->main.stream == b->ctx->stream &&
-                    memcmp(b->last_jobs.data(), jobs, count * sizeof(bntt_job)) == 0;
+  const bool same = !inject && same_list(b->main, jobs, count, b->ctx->stream);
   if (!same) {  // a new list is launched directly; a graph is captured if it comes again
-    b->last_jobs.clear();
+    b->main.staged_raw = nullptr;
     if (int rc = build_schedule_dev(b, b->main, jobs, count, false)) return rc;
     if (int rc = upload(b, b->main, b->ctx->stream, false, false, b->upload_stream)) return rc;
-    if (!inject) b->last_jobs.assign(jobs, jobs + count);
+    if (inject) b->main.staged_raw = nullptr;  // the next run rebuilds without the injected fault
   } else if (int rc = capture(b, b->main)) {
     return rc;
   }
@@ -603,13 +612,11 @@ int bntt_batch_run_inverse_dev(bntt_batch* b, const bntt_job* jobs, size_t count
                "and the default arithmetic");
   for (bntt_plan* p : b->plans)
     if (int rc = plan_ensure_inverse(p)) return rc;
-  const bool same = b->inv_last_jobs.size() == count && b->inv.stream == b->ctx->stream &&
-                    memcmp(b->inv_last_jobs.data(), jobs, count * sizeof(bntt_job)) == 0;
+  const bool same = same_list(b->inv, jobs, count, b->ctx->stream);
   if (!same) {
-    b->inv_last_jobs.clear();
+    b->inv.staged_raw = nullptr;
     if (int rc = build_schedule_dev(b, b->inv, jobs, count, true)) return rc;
     if (int rc = upload(b, b->inv, b->ctx->stream, true, false, b->upload_stream)) return rc;
-    b->inv_last_jobs.assign(jobs, jobs + count);
   } else if (int rc = capture(b, b->inv)) {
     return rc;
   }

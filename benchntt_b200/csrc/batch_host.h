@@ -34,6 +34,11 @@ struct Schedule {
   uint32_t small = 0;                       // jobs of at most 2^10 points
   uint32_t first[11] = {};                  // first position of each small size
   const bntt_job* raw = nullptr;            // the caller's jobs (valid during the upload)
+  // the latest device-built list as copied into pinned staging: a later call
+  // with the same jobs is recognised by comparing with it (the staging buffer
+  // is rewritten only by the upload after next)
+  const bntt_job* staged_raw = nullptr;
+  size_t staged_count = 0;
   std::vector<PlanRef> plan_ref;
   std::vector<LargeRef> large_ref;
   // device copies of djobs, order, items and pass_tiles in one buffer, two
@@ -73,7 +78,6 @@ struct bntt_batch {
   int layout = 0;
   bntt::ShapeChoice shapes{};
   // device-pointer runs
-  std::vector<bntt_job> last_jobs;
   bntt::Schedule main;
   // host-pointer runs: packed device region, job groups with own schedules
   std::vector<bntt_job> host_last_jobs;
@@ -95,7 +99,6 @@ struct bntt_batch {
   // fault injection for tests of the failure path (bntt_batch_inject_wait_timeout)
   uint32_t inject_polls = 0;
   // inverse runs (bntt_batch_run_inverse_dev)
-  std::vector<bntt_job> inv_last_jobs;
   bntt::Schedule inv;
   cudaStream_t upload_stream = nullptr;  // schedule copies of device-pointer runs
 };

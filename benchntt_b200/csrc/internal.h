@@ -65,6 +65,7 @@ struct SubKernel {
   const void* fn;
   int max_blocks_per_sm;  // filled lazily
   int minb;               // __launch_bounds__ minimum resident CTAs
+  int src = 0;            // SRC_STAGED / TW_SHARED (k_ntt_sub_staged), else 0
 };
 
 const std::vector<SubKernel>& sub_kernels();

@@ -74,6 +74,31 @@ struct Epilogue {
   MulB mul;
 };
 
+// Where a tile's first pass finds its inputs and every pass its twiddles.
+//   SRC_STAGED  the inputs were copied into the tile's shared-memory slots
+//               beforehand (cp.async, k_ntt_sub_staged); the first pass
+//               gathers from there like the later passes
+//   TW_SHARED   sr.tw points at a copy of the table in shared memory
+enum : int { SRC_GLOBAL = 0, SRC_STAGED = 1, TW_SHARED = 2 };
+
+// 16-byte asynchronous copy global -> shared (cp.async, L2 only), and the
+// group commit / wait that order them.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
+}
+__device__ __forceinline__ uint4 lds128(const uint4* p) {
+  uint4 v;
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+  return v;
+}
+
 template <int M, int LOGR, int TPC, int MAP, class Arith>
 struct NttTile {
   static constexpr int R = 1 << LOGR;
@@ -117,15 +142,15 @@ struct NttTile {
   // Runs the whole sub-transform.  Every thread of the tile must call it
   // (it synchronises); threads whose sub-transform is not valid compute on
   // zeros and store nothing.
-  template <int LDP>
+  template <int LDP, int SRC = SRC_GLOBAL>
   __device__ __forceinline__ static void run(const SubRef& sr, int sub, int lane, uint4* smem,
                                              const ModParams& mp, int layout,
                                              const MulB& mb = MulB{}) {
     U128 v[R];
-    pass<0, LDP>(v, sr, sub, lane, smem, mp, layout, mb);
+    pass<0, LDP, SRC>(v, sr, sub, lane, smem, mp, layout, mb);
   }
 
-  template <int P, int LDP>
+  template <int P, int LDP, int SRC = SRC_GLOBAL>
   __device__ __forceinline__ static void pass(U128 (&v)[R], const SubRef& sr, int sub, int lane,
                                               uint4* smem, const ModParams& mp, int layout,
                                               const MulB& mb) {
@@ -144,7 +169,9 @@ struct NttTile {
 #pragma unroll
       for (int j = 0; j < G; ++j) {
         const int idx = base | (j << lo);
-        if constexpr (P == 0) {
+        if constexpr (P == 0 && (SRC & SRC_STAGED) != 0) {
+          v[i * G + j] = from_mem(smem[slot(sub, idx)], layout);  // staged in memory order
+        } else if constexpr (P == 0) {
           if (sr.valid) {
             v[i * G + j] = from_mem(ld_data<LDP>(sr.x + ((size_t)idx << sr.lshift)), layout);
           } else {
@@ -169,7 +196,8 @@ struct NttTile {
 #pragma unroll
         for (int u = 0; u < (1 << t); ++u) {
           // tables are stored in limb order (LAYOUT_U128) by the plan
-          const uint4 tv = __ldg(sr.tw + ((gt << t) + (uint32_t)u));
+          const uint4 tv = (SRC & TW_SHARED) != 0 ? lds128(sr.tw + ((gt << t) + (uint32_t)u))
+                                                  : __ldg(sr.tw + ((gt << t) + (uint32_t)u));
           const U128 w = U128{{tv.x, tv.y, tv.z, tv.w}};
 #pragma unroll
           for (int k = 0; k < half; ++k) {
@@ -206,7 +234,7 @@ struct NttTile {
     }
     if constexpr (P + 1 < NPASS) {
       sync();
-      pass<P + 1, LDP>(v, sr, sub, lane, smem, mp, layout, mb);
+      pass<P + 1, LDP, SRC>(v, sr, sub, lane, smem, mp, layout, mb);
     }
   }
 };

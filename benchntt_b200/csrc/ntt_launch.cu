@@ -15,6 +15,7 @@ void append_fast_il(std::vector<SubKernel>& v);
 void append_ref(std::vector<SubKernel>& v);
 void append_fast_occ(std::vector<SubKernel>& v);
 void append_fast_small(std::vector<SubKernel>& v);
+void append_fast_staged(std::vector<SubKernel>& v);
 
 const std::vector<SubKernel>& sub_kernels() {
   static std::vector<SubKernel> v = [] {
@@ -25,6 +26,7 @@ const std::vector<SubKernel>& sub_kernels() {
     append_ref(r);
     append_fast_occ(r);
     append_fast_small(r);
+    append_fast_staged(r);
     return r;
   }();
   return v;
@@ -141,6 +143,9 @@ int plan_choose_kernels(bntt_plan* p) {
     // the tuned shape if the autotuner ran, else the first registered shape
     // that fits (interleaved tiles need TPC adjacent columns, so TPC <= 2^l)
     const SubKernel* k = tuned_sub_kernel(m, map, fast ? 1 : 0, l);
+    // a table copied into shared memory holds entries below 2^m only: whole
+    // transforms (s0 = 0)
+    if (k && (k->src & TW_SHARED) && s0 != 0) k = nullptr;
     // untuned contiguous passes with the fast multiply: the 4-element shape
     // capped at 4 resident CTAs per SM (2^3..2^10), else the shape capped at
     // 3 -- measured on B200; without a cap the compiler spends up to 214
@@ -148,12 +153,12 @@ int plan_choose_kernels(bntt_plan* p) {
     for (int want_minb : {4, 3}) {
       for (const SubKernel& c : sub_kernels()) {
         if (k || map != MAP_CONTIG || !fast) break;
-        if (c.m == m && c.map == map && c.fast == 1 && c.minb == want_minb) k = &c;
+        if (c.m == m && c.map == map && c.fast == 1 && c.minb == want_minb && c.src == 0) k = &c;
       }
     }
     for (const SubKernel& c : sub_kernels()) {
       if (k) break;
-      if (c.m != m || c.map != map || c.fast != (fast ? 1 : 0)) continue;
+      if (c.m != m || c.map != map || c.fast != (fast ? 1 : 0) || c.src != 0) continue;
       if (map == MAP_INTERLEAVED && (1 << l) < c.tpc) continue;
       k = &c;
     }

@@ -405,8 +405,10 @@ int bntt_server_replay_ex(bntt_server *srv, const bntt_request *reqs, size_t n, 
 
 /* ------------------------------------------------------------- autotuner */
 /* Times every compiled kernel shape for transform sizes 2^1..2^10 (register
- * tile of 8 or 16 elements per thread = radix and number of shared-memory
- * passes, transforms per CTA, two or three resident CTAs per SM), the strided
+ * tile of 4, 8 or 16 elements per thread = radix and number of shared-memory
+ * passes, transforms per CTA, two to four resident CTAs per SM, inputs read
+ * by the first pass or staged into shared memory a tile ahead, twiddles read
+ * through L1 or from a copy of the table in shared memory), the strided
  * first pass of large transforms, and the persistent kernel's tile shape per
  * size, on this device; the fastest become the defaults of plans and batches
  * created afterwards in this process.  Writes the choices to `path` if it is

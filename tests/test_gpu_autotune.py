@@ -79,3 +79,65 @@ def test_tuned_batch_bit_exact(tuned):
     eng.close()
     for p in plans.values():
         p.close()
+
+
+def _force(ctx, tmp_path, head: str, lines: list[str]):
+    """Installs exactly the given tuner choices (a hand-written tune file)."""
+    f = tmp_path / "forced.tune"
+    f.write_text(head + "".join(l + "\n" for l in lines))
+    bn.lib().bntt_autotune_reset()
+    ctx.autotune_load(str(f))
+
+
+@pytest.mark.parametrize("src", [1, 3], ids=["staged", "staged_table_in_smem"])
+@pytest.mark.parametrize("logn", list(range(3, 11)))
+def test_staged_shapes_bit_exact(tuned, tmp_path, logn, src):
+    """The kernels whose inputs are staged into shared memory a tile ahead
+    (and whose table sits in shared memory, src=3), forced through a tune
+    file: more tiles than CTAs (the copy of the next tile overlaps the
+    current one) and a partial last tile, against the oracle."""
+    ctx, path = tuned
+    head = open(path).readline()
+    tpc = 1024 >> logn
+    _force(ctx, tmp_path, head, [f"sub {logn} 0 1 2 {tpc} 4 {src}"])
+    n = 1 << logn
+    batch = (2 * 4 * ctx.sm_count + 5) * tpc + 3
+    x = C.uniform_pairs(40 + logn, n * batch, C.Q_NTT)
+    t = C.uniform_pairs(41 + logn, n, C.Q_NTT)
+    plan = bn.Plan(ctx, logn, C.Q_NTT, C.MU_NTT, t)
+    y = np.empty_like(x)
+    plan.forward(y, x)
+    assert np.array_equal(y, C.oracle_ntt(x, t, logn, threads=8))
+    plan.close()
+    ctx.autotune_load(path)   # the measured choices again, for the other tests
+
+
+@pytest.mark.parametrize("src", [1, 3])
+def test_staged_fused_product_and_u128_layout(tuned, tmp_path, src):
+    """The staged kernels with the fused pointwise product and with native
+    uint128_t buffers."""
+    import torch
+    ctx, path = tuned
+    head = open(path).readline()
+    _force(ctx, tmp_path, head, [f"sub 7 0 1 2 8 4 {src}"])
+    logn, n, batch = 7, 128, 5001
+    x = C.uniform_pairs(51, n * batch, C.Q_NTT)
+    b = C.uniform_pairs(52, n * batch, C.Q_NTT)
+    t = C.uniform_pairs(53, n, C.Q_NTT)
+    plan = bn.Plan(ctx, logn, C.Q_NTT, C.MU_NTT, t)
+    dx = torch.from_numpy(x.view(np.int64)).cuda()
+    db = torch.from_numpy(b.view(np.int64)).cuda()
+    dy = torch.empty_like(dx)
+    plan.forward_mul(dy, dx, db, True, batch)
+    torch.cuda.synchronize()
+    want = C.oracle_blas("vvmul", C.oracle_ntt(x, t, logn, threads=8), b, C.Q_NTT, C.MU_NTT)
+    assert np.array_equal(dy.cpu().numpy().view(np.uint64), want)
+    plan.close()
+    # the same transform on native little-endian uint128_t buffers
+    plan = bn.Plan(ctx, logn, C.Q_NTT, C.MU_NTT, np.ascontiguousarray(t[:, ::-1]), layout=bn.LAYOUT_U128)
+    xu = np.ascontiguousarray(x[:, ::-1])
+    yu = np.empty_like(xu)
+    plan.forward(yu, xu)
+    assert np.array_equal(yu[:, ::-1], C.oracle_ntt(x, t, logn, threads=8))
+    plan.close()
+    ctx.autotune_load(path)
