@@ -1,9 +1,9 @@
 """Regenerates the committed parity fixtures in tests/golden/.
 
-Run in a checkout that has the benchNTT sources (default /root/reference, or
-BNTT_REF_ROOT) and the reference built in place (`make -C oracle ref`):
+Run with BNTT_REF_ROOT naming the benchNTT source tree, after building the
+reference in place (`make -C oracle ref REF_ROOT=$BNTT_REF_ROOT`):
 
-    python tests/golden/make_golden.py
+    BNTT_REF_ROOT=<benchNTT> python tests/golden/make_golden.py
 
 Writes:
   ref_data.npz   the reference's own golden vectors, converted from text:
@@ -40,7 +40,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 import common as C  # noqa: E402
 
-REF_ROOT = os.environ.get("BNTT_REF_ROOT", "/root/reference")
+REF_ROOT = os.environ.get("BNTT_REF_ROOT", "")
 
 # Seeds of the generated fixtures (tests regenerate the same inputs).
 SEED_X = 1000
@@ -66,6 +66,8 @@ def gen_inputs(logn: int, q: int = C.Q_NTT):
 
 
 def main() -> None:
+    if not REF_ROOT or not os.path.isdir(os.path.join(REF_ROOT, "data")):
+        sys.exit("set BNTT_REF_ROOT to the benchNTT source tree (the directory holding data/ and src/)")
     data = os.path.join(REF_ROOT, "data")
     out = {}
     for logn in range(4, 11):
