@@ -559,21 +559,17 @@ def fresh_lists(args, ctx, stream, engine, jobs, batch, batched_value) -> dict:
     wall = (time.perf_counter() - t0) / steps
     ms = e0.elapsed_time(e1) / steps
     # the host's own work per new list: the call timed with the device idle
-    # (nothing to wait for), and the device's time for that step alone
-    host, dev = [], []
+    # (nothing to wait for)
+    host = []
     for i in range(6):
         ctx.synchronize()
-        e0.record(stream)
         t1 = time.perf_counter()
         engine.run_dev(lists[i % 2])
         host.append(time.perf_counter() - t1)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        dev.append(e0.elapsed_time(e1))
+    ctx.synchronize()
     return {"value": batch.count / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
             "host_wall_ms_per_step": wall * 1e3, "vs_same_list": batch.count / (ms * 1e-3) / batched_value,
-            "host_ms_per_new_list": statistics.median(host) * 1e3,
-            "device_ms_per_new_list_alone": statistics.median(dev)}
+            "host_ms_per_new_list": statistics.median(host) * 1e3}
 
 
 def per_call(args, dist, ctx, stream, engine, jobs, units, batched_value) -> dict:

@@ -411,24 +411,26 @@ static int upload(bntt_batch* b, Schedule& sc, cudaStream_t stream, bool inverse
   char* d = static_cast<char*>(sc.d_sched[set]);
   BNTT_CK(cudaMemcpyAsync(d, h, staged, cudaMemcpyHostToDevice, cs));
   BNTT_CK(cudaEventRecord(sc.stage_done[si], cs));
+  // descriptors and size order, built on the device after the copy, on the
+  // copy's stream: the build runs while earlier launches finish (it writes
+  // only the buffer they do not read), off the path between two launches
+  if (sc.dev_build && sc.count) {
+    BNTT_CK(cudaMemsetAsync(d + o_fill, 0, 256, cs));
+    if (int rc = launch_build_jobs(reinterpret_cast<const bntt_job*>(d + o_raw), sc.count,
+                                   reinterpret_cast<const PlanRef*>(d + o_plan),
+                                   reinterpret_cast<const LargeRef*>(d + o_large),
+                                   (uint32_t)sc.large_ref.size(), sc.first, reinterpret_cast<uint32_t*>(d + o_fill),
+                                   reinterpret_cast<DevJob*>(d + o_jb), reinterpret_cast<uint32_t*>(d + o_ob), cs))
+      return rc;
+    c->launches++;
+    b->last_launches++;
+  }
   if (cs != stream) {
     if (!sc.set_ready) BNTT_CK(cudaEventCreateWithFlags(&sc.set_ready, cudaEventDisableTiming));
     BNTT_CK(cudaEventRecord(sc.set_ready, cs));
     BNTT_CK(cudaStreamWaitEvent(stream, sc.set_ready, 0));
   }
   sc.cur = set;
-  if (sc.dev_build && sc.count) {  // descriptors and size order, on the device, before the launches
-    BNTT_CK(cudaMemsetAsync(d + o_fill, 0, 256, stream));
-    if (int rc = launch_build_jobs(reinterpret_cast<const bntt_job*>(d + o_raw), sc.count,
-                                   reinterpret_cast<const PlanRef*>(d + o_plan),
-                                   reinterpret_cast<const LargeRef*>(d + o_large),
-                                   (uint32_t)sc.large_ref.size(), sc.first, reinterpret_cast<uint32_t*>(d + o_fill),
-                                   reinterpret_cast<DevJob*>(d + o_jb), reinterpret_cast<uint32_t*>(d + o_ob),
-                                   stream))
-      return rc;
-    c->launches++;
-    b->last_launches++;
-  }
   if (sticky_err) BNTT_CK(cudaMemsetAsync(sc.d_ctl, 0, cb, stream));
   sc.stream = stream;
   sc.inverse = inverse;
