@@ -346,7 +346,7 @@ def run_ours(args, dist: Dist):
                 "peak_gbs": peaks.get("hbm_gbs"), "algorithmic_bytes": alg_bytes,
                 "frac": (alg_bytes / (ms_local * 1e-3) / 1e9) / peaks["hbm_gbs"]
                 if peaks.get("hbm_gbs") else None,
-                "peak_source": "MEASURED_PEAKS.json" if peaks.get("from_file") else "fallback"},
+                "peak_source": peaks["source"]},
     }
 
     result = {
@@ -407,13 +407,42 @@ def butterfly_ceiling(ctx, bfly: int, ms: float) -> dict:
             "frac": achieved / peak, "peak_source": "measured live: bntt_probe_butterfly_peak"}
 
 
+_PEAKS = None
+
+
 def measured_peaks() -> dict:
+    """MEASURED_PEAKS.json when the file is present, else the HBM copy
+    bandwidth measured here (a device-to-device copy of 1 GiB, read plus
+    write bytes over its time, best of 5)."""
+    global _PEAKS
+    if _PEAKS is not None:
+        return _PEAKS
     try:
         d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         d["from_file"] = True
-        return d
+        d["source"] = "MEASURED_PEAKS.json"
     except (OSError, ValueError):
-        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "from_file": False}
+        d = {"hbm_gbs": live_copy_gbs(), "from_file": False,
+             "source": "measured live: device-to-device copy of 1 GiB (read + write bytes)"}
+    _PEAKS = d
+    return d
+
+
+def live_copy_gbs() -> float:
+    import torch
+    a = torch.empty(1 << 30, dtype=torch.uint8, device="cuda")
+    b = torch.empty_like(a)
+    a.fill_(1)
+    best = 1e30
+    for _ in range(6):
+        e0, e1 = cuda_events()
+        e0.record()
+        b.copy_(a)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2 * (1 << 30) / (best * 1e-3) / 1e9
 
 
 def e2e_uneven(args, dist, ctx, engine, batch, pid, units: int) -> dict:
@@ -606,7 +635,7 @@ def blas_bench(args, ctx, stream, peaks) -> dict:
     bn.check(L.bntt_fill_uniform_dev(ctx.handle, b.data_ptr(), n, 4000, 0, ctypes.byref(mod), 0))
     res = {"length": n, "bytes_per_op": HBM_BYTES_PER_ELEM_BLAS * n,
            "peak_gbs": peaks.get("hbm_gbs"),
-           "peak_source": "MEASURED_PEAKS.json" if peaks.get("from_file") else "fallback",
+           "peak_source": peaks["source"],
            "note": "operands 256 MiB each > L2: no flush needed"}
     for op in ("vvadd", "vvsub", "vvmul", "axpy"):
         fn = getattr(L, f"bntt_{op}_dev")
@@ -1036,39 +1065,47 @@ def run_reference(args, dist: Dist):
 
 def summary(res: dict) -> dict:
     """The figures of the secondary configurations, compact, as the last key
-    of the line."""
+    of the line (rows are lists; "fields" names their entries)."""
+    r = lambda v, d=1: None if v is None else round(v, d)
     out = {}
     blas = res.get("blas", {})
     if blas:
-        out["blas_2^24"] = {op: {"gbs": round(v["gbs"]), "hbm_frac": round(v["frac_of_hbm_peak"], 3),
-                                 "e2e_gbs": round(v["e2e_host"]["gbs"], 1) if "e2e_host" in v else None,
-                                 "cpu_gbs": round(v["cpu_reference_gbs"], 1) if "cpu_reference_gbs" in v else None}
-                            for op, v in blas.items() if isinstance(v, dict) and "gbs" in v}
+        out["blas_2^24"] = {"fields": ["GB/s", "hbm_frac", "e2e_host_GB/s", "cpu_ref_GB/s"]}
+        for op, v in blas.items():
+            if isinstance(v, dict) and "gbs" in v:
+                out["blas_2^24"][op] = [round(v["gbs"]), r(v["frac_of_hbm_peak"], 3),
+                                        r(v.get("e2e_host", {}).get("gbs")), r(v.get("cpu_reference_gbs"))]
     pc = res.get("per_call")
     if pc:
-        out["per_call"] = {"ntt_per_s": round(pc["value"]), "batched_over_per_call": round(pc["batched_over_per_call"], 1)}
+        out["per_call"] = {"ntt_per_s": round(pc["value"]), "batched_over_per_call": r(pc["batched_over_per_call"])}
+    nl = res.get("new_job_list_each_step")
+    if nl:
+        out["new_list_vs_same"] = r(nl["vs_same_list"], 3)
     uni = res.get("uniform")
     if uni:
-        out["uniform_65536"] = {n: {"one_launch": round(v["ntt_per_s"]),
-                                    "per_transform": round(v["per_transform_ntt_per_s"])
-                                    if "per_transform_ntt_per_s" in v else None,
-                                    "imad80": round(v["imad80_frac"], 2),
-                                    "cpu": round(v["cpu_reference_ntt_per_s"]) if "cpu_reference_ntt_per_s" in v else None}
-                                for n, v in uni.items()}
+        out["uniform_65536"] = {"fields": ["one_launch_M/s", "per_transform_M/s", "imad80_frac", "cpu_ref_M/s"]}
+        for n, v in uni.items():
+            m = v["ntt_per_s"] / 1e6
+            out["uniform_65536"][n] = [r(m, 1 if m >= 10 else 4), r(v.get("per_transform_ntt_per_s", 0) / 1e6, 3)
+                                       if "per_transform_ntt_per_s" in v else None, r(v["imad80_frac"], 3),
+                                       r(v.get("cpu_reference_ntt_per_s", 0) / 1e6, 3)
+                                       if "cpu_reference_ntt_per_s" in v else None]
     sv = res.get("serving")
     if sv:
-        out["serving"] = {k: {"rate": v["rate_req_s"], "cb_p99_ms": round(v["continuous_batching"]["p99_ms"], 3),
-                              "serial_p99_ms": round(v["one_call_at_a_time"]["p99_ms"], 3),
-                              "p99_speedup": round(v["p99_speedup"], 1),
-                              "cb_service_p99_ms": round(v["continuous_batching"]["service_p99_ms"], 3),
-                              "serial_service_p99_ms": round(v["one_call_at_a_time"]["service_p99_ms"], 3)}
-                          for k, v in sv.items() if isinstance(v, dict) and "p99_speedup" in v}
+        out["serving"] = {"fields": ["rate", "cb_p99_ms", "serial_p99_ms", "p99_speedup", "cb_service_p99_ms",
+                                     "serial_service_p99_ms"]}
+        for k, v in sv.items():
+            if isinstance(v, dict) and "p99_speedup" in v:
+                out["serving"][k] = [v["rate_req_s"], r(v["continuous_batching"]["p99_ms"], 3),
+                                     r(v["one_call_at_a_time"]["p99_ms"], 3), r(v["p99_speedup"]),
+                                     r(v["continuous_batching"]["service_p99_ms"], 3),
+                                     r(v["one_call_at_a_time"]["service_p99_ms"], 3)]
     cb = res.get("cpu_baseline")
     if cb:
         out["cpu"] = {"ntt_only": round(cb["value"]), "full_sequence": round(cb["full_sequence"]["value"]),
                       "threads": cb["threads"], "physical_cores": cb["physical_cores"], "smt": cb["smt"],
-                      "gpu_over_cpu": round(res["value"] / cb["value"], 1),
-                      "e2e_over_cpu": round(res["e2e"]["value"] / cb["value"], 2) if "e2e" in res else None}
+                      "gpu_over_cpu": r(res["value"] / cb["value"]),
+                      "e2e_over_cpu": r(res["e2e"]["value"] / cb["value"], 2) if "e2e" in res else None}
     return out
 
 

@@ -54,15 +54,18 @@ static std::string device_key(bntt_ctx* c) {
   return buf;
 }
 
-// time one kernel over a geometry: median of `reps` launches
+// time one kernel over a geometry: median of `reps` launches; with `flush`
+// (a buffer larger than L2) the L2 is overwritten before each timed launch,
+// so inputs that would fit in it come from HBM as in a first use
 static int time_sub(bntt_ctx* c, const SubKernel* k, const SubGeom& g, const ModParams& mp, int reps,
-                    float* out_ms) {
+                    float* out_ms, void* flush = nullptr, size_t flush_bytes = 0) {
   cudaEvent_t e0, e1;
   BNTT_CK(cudaEventCreate(&e0));
   BNTT_CK(cudaEventCreate(&e1));
   std::vector<float> t;
   int rc = BNTT_OK;
   for (int r = 0; r < reps + 1 && !rc; ++r) {
+    if (flush) cudaMemsetAsync(flush, r & 0xff, flush_bytes, c->stream);
     cudaEventRecord(e0, c->stream);
     rc = launch_sub(c, k, &g, mp, BNTT_LAYOUT_HILO, c->stream);
     cudaEventRecord(e1, c->stream);
@@ -92,17 +95,21 @@ extern "C" {
 // tiles and, for 2^5..2^10, the strided first HBM pass of large transforms),
 // and the persistent kernel's tile shape per size; installs the fastest as
 // defaults.  If `path` is non-NULL the choices are also written there.
-// Takes a few seconds and about 512 MiB of device memory.
+// Contiguous shapes are timed on batches of 65,536 transforms (at most 2^24
+// elements) with the L2 flushed before each launch: the size of a uniform
+// batch, whose small transforms fit in L2 only when reused.
+// Takes a few seconds and about 1 GiB of device memory.
 int bntt_autotune(bntt_ctx* c, const char* path) {
   BNTT_REQUIRE(c, "ctx is NULL");
   if (int rc = ctx_use_device(c)) return rc;
   const size_t elems = (size_t)1 << 24;  // 256 MiB per buffer: larger than L2
-  void *x = nullptr, *y = nullptr, *tw = nullptr;
+  void *x = nullptr, *y = nullptr, *tw = nullptr, *flush = nullptr;
   int rc;
   if ((rc = ctx_alloc(c, &x, elems * 16)) || (rc = ctx_alloc(c, &y, elems * 16)) ||
-      (rc = ctx_alloc(c, &tw, elems * 16))) {
+      (rc = ctx_alloc(c, &tw, elems * 16)) || (rc = ctx_alloc(c, &flush, elems * 16))) {
     ctx_free(c, x);
     ctx_free(c, y);
+    ctx_free(c, tw);
     return rc;
   }
   const bntt_modulus mod = bntt_modulus_ntt_reference();
@@ -135,7 +142,13 @@ int bntt_autotune(bntt_ctx* c, const char* path) {
           g.m = (uint32_t)m;
           g.nsub = elems >> m;
           float ms = 0;
-          if ((rc = time_sub(c, &k, g, mp, 5, &ms)) != 0) break;
+          if (map == MAP_CONTIG) {
+            g.nsub = std::min<uint64_t>(g.nsub, 65536);
+            rc = time_sub(c, &k, g, mp, 5, &ms, flush, elems * 16);
+          } else {
+            rc = time_sub(c, &k, g, mp, 5, &ms);
+          }
+          if (rc) break;
           char line[160];
           snprintf(line, sizeof(line), "# sub m=%d map=%d fast=%d logr=%d tpc=%d minb=%d src=%d %.4f ms\n",
                    m, map, fast, k.logr, k.tpc, k.minb, k.src, ms);
@@ -193,6 +206,7 @@ int bntt_autotune(bntt_ctx* c, const char* path) {
   ctx_free(c, x);
   ctx_free(c, y);
   ctx_free(c, tw);
+  ctx_free(c, flush);
   if (rc) return rc;
   if (path) {
     FILE* f = fopen(path, "w");
@@ -222,12 +236,16 @@ int bntt_autotune_load(bntt_ctx* c, const char* path) {
     int m, map, fast, logr, tpc, minb, src = 0;
     const int got = sscanf(line, "sub %d %d %d %d %d %d %d", &m, &map, &fast, &logr, &tpc, &minb, &src);
     if (got == 6 || got == 7) {  // files without the last field name an unstaged shape
+      bool found = false;
       for (const SubKernel& k : sub_kernels())
         if (k.m == m && k.map == map && k.fast == fast && k.logr == logr && k.tpc == tpc && k.minb == minb &&
             k.src == src) {
           std::lock_guard<std::mutex> g(g_tune_mu);
           g_sub_choice[m][map][fast] = &k;
+          found = true;
         }
+      if (!found)
+        rc = set_error(BNTT_EINVAL, "%s names a kernel shape this library does not have: %s", path, line);
     } else if (sscanf(line, "batch %d %d %d", &m, &logr, &tpc) == 3) {
       for (int s = 0; s < batch_shape_count(); ++s) {
         int sm, slogr, stpc, smap;

@@ -16,6 +16,7 @@ void append_ref(std::vector<SubKernel>& v);
 void append_fast_occ(std::vector<SubKernel>& v);
 void append_fast_small(std::vector<SubKernel>& v);
 void append_fast_staged(std::vector<SubKernel>& v);
+void append_fast_occ5(std::vector<SubKernel>& v);
 
 const std::vector<SubKernel>& sub_kernels() {
   static std::vector<SubKernel> v = [] {
@@ -27,6 +28,7 @@ const std::vector<SubKernel>& sub_kernels() {
     append_fast_occ(r);
     append_fast_small(r);
     append_fast_staged(r);
+    append_fast_occ5(r);
     return r;
   }();
   return v;

@@ -412,11 +412,14 @@ int bntt_server_replay_ex(bntt_server *srv, const bntt_request *reqs, size_t n, 
  * first pass of large transforms, and the persistent kernel's tile shape per
  * size, on this device; the fastest become the defaults of plans and batches
  * created afterwards in this process.  Writes the choices to `path` if it is
- * not NULL.  A few seconds; about 768 MiB of device memory while it runs.
+ * not NULL.  Contiguous shapes are timed on 65,536 transforms (at most 2^24
+ * elements) with the L2 flushed before each launch.  A few seconds; about
+ * 1 GiB of device memory while it runs.
  * The reference fixes one scalar / SIMD code path per size at compile time
  * (src/ntt_scalar.c:21, benchmark/run_ntt.sh); no counterpart there. */
 int bntt_autotune(bntt_ctx *ctx, const char *path);
-/* Installs choices saved by bntt_autotune (refused for another device). */
+/* Installs choices saved by bntt_autotune (refused for another device, or
+ * when a line names a kernel shape this build does not have). */
 int bntt_autotune_load(bntt_ctx *ctx, const char *path);
 /* Drops tuned choices; compiled defaults apply to new plans and batches. */
 int bntt_autotune_reset(void);

@@ -89,19 +89,26 @@ def _force(ctx, tmp_path, head: str, lines: list[str]):
     ctx.autotune_load(str(f))
 
 
-@pytest.mark.parametrize("src", [1, 3], ids=["staged", "staged_table_in_smem"])
-@pytest.mark.parametrize("logn", list(range(3, 11)))
-def test_staged_shapes_bit_exact(tuned, tmp_path, logn, src):
-    """The kernels whose inputs are staged into shared memory a tile ahead
-    (and whose table sits in shared memory, src=3), forced through a tune
-    file: more tiles than CTAs (the copy of the next tile overlaps the
-    current one) and a partial last tile, against the oracle."""
+# (log2n, logr, tpc, minb, src): the staged kernels (inputs staged into
+# shared memory a tile ahead; src=3 also holds the table there) at 4 and 5
+# resident CTAs per SM, the 48-register plain shapes and 8 elements per thread
+# at 2^4
+SHAPES = ([(m, 2, 1024 >> m, 4, src) for m in range(3, 11) for src in (1, 3)] +
+          [(m, 2, 1024 >> m, 5, src) for m in range(3, 9) for src in (0, 1, 3)] +
+          [(4, 3, 128, 4, 0)])
+
+
+@pytest.mark.parametrize("logn,logr,tpc,minb,src", SHAPES, ids=lambda v: str(v))
+def test_candidate_shapes_bit_exact(tuned, tmp_path, logn, logr, tpc, minb, src):
+    """Every small-transform candidate the tuner can pick, forced through a
+    tune file: more tiles than CTAs (for staged kernels the copy of the next
+    tile overlaps the current one) and a partial last tile, against the
+    oracle."""
     ctx, path = tuned
     head = open(path).readline()
-    tpc = 1024 >> logn
-    _force(ctx, tmp_path, head, [f"sub {logn} 0 1 2 {tpc} 4 {src}"])
+    _force(ctx, tmp_path, head, [f"sub {logn} 0 1 {logr} {tpc} {minb} {src}"])
     n = 1 << logn
-    batch = (2 * 4 * ctx.sm_count + 5) * tpc + 3
+    batch = (2 * minb * ctx.sm_count + 5) * tpc + 3
     x = C.uniform_pairs(40 + logn, n * batch, C.Q_NTT)
     t = C.uniform_pairs(41 + logn, n, C.Q_NTT)
     plan = bn.Plan(ctx, logn, C.Q_NTT, C.MU_NTT, t)
