@@ -87,6 +87,21 @@ struct NttEngine {
     constexpr int G = 1 << r, GPT = R / G;
     const int hi_mask = ~((1 << lo) - 1);
     const int step = lay.lmul << lo;  // linear-index distance of j and j + 1
+    // Slot of element j of a group: pad(lb + j*step).  With 4 elements per
+    // thread it is pad(lb) plus an offset that does not depend on lb, so each
+    // element costs one add: step a multiple of 8 (interleaved tiles, whose
+    // lmul is a multiple of 8, and contiguous passes with lo >= 3) adds step
+    // plus its pad slots; contiguous passes with lo <= 2 start a group at a
+    // linear index whose position in its 8-slot block leaves room for the
+    // group up to one pad slot, crossed between elements 1 and 2 when the
+    // step is 4 (the group base is (g mod 2^lo) + (g >> lo) * G * 2^lo on top
+    // of a multiple of 8).
+    const int s9 = step >= 8 ? step + (step >> 3) : step;
+    const int c2 = step == 4 ? 1 : 0;
+    auto slot_of = [&](int lb, int j) {
+      if constexpr (LOGR == 2) return pad(lb) + j * s9 + (j >> 1) * c2;
+      else return pad(lb + j * step);
+    };
     const uint32_t gstep = 1u << (lo + sr.lshift);  // the same in global memory
     // group i's local index base: (g & lomask) | ((g >> lo) << (lo + r))
     auto base = [&](int i) {
@@ -111,7 +126,7 @@ struct NttEngine {
         const int lb = lay.lbase + base(i) * lay.lmul;
 #pragma unroll
         for (int j = 0; j < G; ++j) {
-          const uint4 t = smem[pad(lb + j * step)];
+          const uint4 t = smem[slot_of(lb, j)];
           v[i * G + j] = U128{{t.x, t.y, t.z, t.w}};
         }
       }
@@ -175,7 +190,7 @@ struct NttEngine {
 #pragma unroll
         for (int j = 0; j < G; ++j) {
           const U128& e = v[i * G + j];
-          smem[pad(lb + j * step)] =
+          smem[slot_of(lb, j)] =
               make_uint4(e.w[0], e.w[1], e.w[2], e.w[3]);
         }
       }
