@@ -71,6 +71,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (profiling captures: no tuning launches first)")
+    ap.add_argument("--tune-save", default=None, help="write the autotuner's choices to this file")
+    ap.add_argument("--tune-load", default=None,
+                    help="install choices saved earlier instead of tuning (profiling captures)")
     return ap.parse_args()
 
 
@@ -242,6 +245,8 @@ def run_only(args, dist: Dist):
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(device=dev)
     ctx = bn.Context(dev, stream=stream.cuda_stream)
+    if args.tune_load:
+        ctx.autotune_load(args.tune_load)
     if args.only in ("uniform", "inverse"):
         res = uniform_bench(args, ctx, stream, ctx.imad_peak(), sizes=[args.logn],
                             inverse=args.only == "inverse")
@@ -271,9 +276,15 @@ def run_ours(args, dist: Dist):
     tune_path = os.path.join(tempfile.mkdtemp(), "bntt.tune")
     t_tune = time.perf_counter()
     tuned = []
-    if not args.no_tune:
+    if args.tune_load:
+        ctx.autotune_load(args.tune_load)
+        tuned = [l.strip() for l in open(args.tune_load) if l.startswith(("sub ", "batch "))]
+    elif not args.no_tune:
         ctx.autotune(tune_path)
         tuned = [l.strip() for l in open(tune_path) if l.startswith(("sub ", "batch "))]
+        if args.tune_save:
+            import shutil
+            shutil.copy(tune_path, args.tune_save)
     tune_s = time.perf_counter() - t_tune
 
     # ---------------------------------------------------- headline workload

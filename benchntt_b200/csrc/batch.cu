@@ -16,12 +16,12 @@ namespace bntt {
 const void* batch_kernel_fast_minb(int minb);
 const void* batch_kernel_ref();
 
-// Resident CTAs per SM the fast batch kernel is compiled for (2, 3 or 4,
+// Resident CTAs per SM the fast batch kernel is compiled for (2 to 5,
 // default 4), read once at start-up from BNTT_BATCH_MINB.
 static const int g_batch_minb = [] {
   const char* e = getenv("BNTT_BATCH_MINB");
   const int v = e ? atoi(e) : 4;
-  return v == 2 || v == 3 ? v : 4;
+  return v == 2 || v == 3 || v == 5 ? v : 4;
 }();
 
 size_t shape_smem(int s) {

@@ -208,8 +208,13 @@ __device__ __forceinline__ void item_publish(const WorkItem& it, const BatchArgs
   }
 }
 
+// The item functions are templates on the kernel's MINB as well: a
+// non-inlined function is compiled once for all its callers, at the smallest
+// register budget among them, so a kernel variant with more resident CTAs
+// would otherwise make every variant's items spill.
+
 // Sizes 2^1, 2^2: one thread per transform, fully unrolled.
-template <int M, class Arith>
+template <int M, class Arith, int MINB>
 __device__ __noinline__ void run_item_tiny(const WorkItem& it, const BatchArgs& ba, uint4* smem,
                                            const ModParams& mp, int layout, int* s_flag) {
   using T = NttTile<M, M, kBatchThreads, MAP_CONTIG, Arith>;
@@ -221,7 +226,7 @@ __device__ __noinline__ void run_item_tiny(const WorkItem& it, const BatchArgs& 
 }
 
 // Every other shape: the runtime-size engine.
-template <class Arith>
+template <class Arith, int MINB>
 __device__ __noinline__ void run_item_engine(const WorkItem& it, const BatchArgs& ba, uint4* smem,
                                              const ModParams& mp, int layout, int* s_flag) {
   using E = NttEngine<kBatchLogR, Arith>;
@@ -247,7 +252,7 @@ __device__ __noinline__ void run_item_engine(const WorkItem& it, const BatchArgs
 // 2^9 +7 %, 2^8 +7 %, 2^20 jobs +9 %).  Specialising the smaller and the other
 // interleaved shapes as well made the kernel 5 % slower overall (a larger
 // kernel), so they stay on the engine.
-template <int M, int TPC, int MAP, class Arith>
+template <int M, int TPC, int MAP, class Arith, int MINB>
 __device__ __noinline__ void run_item_tile(const WorkItem& it, const BatchArgs& ba, uint4* smem,
                                            const ModParams& mp, int layout, int* s_flag) {
   using T = NttTile<M, kBatchLogR, TPC, MAP, Arith>;
@@ -271,14 +276,14 @@ __global__ void __launch_bounds__(kBatchThreads, MINB) k_batch(BatchArgs ba, Mod
     const uint32_t i = s_item;
     if (i >= ba.nitems) break;
     const WorkItem it = ba.items[i];
-    if (it.shape == 0) run_item_tiny<1, Arith>(it, ba, smem, mp, layout, &s_flag);
-    else if (it.shape == 1) run_item_tiny<2, Arith>(it, ba, smem, mp, layout, &s_flag);
-    else if (it.shape == 9) run_item_tile<10, 1, MAP_CONTIG, Arith>(it, ba, smem, mp, layout, &s_flag);
-    else if (it.shape == 8) run_item_tile<9, 2, MAP_CONTIG, Arith>(it, ba, smem, mp, layout, &s_flag);
-    else if (it.shape == 7) run_item_tile<8, 4, MAP_CONTIG, Arith>(it, ba, smem, mp, layout, &s_flag);
-    else if (it.shape == 6) run_item_tile<7, 8, MAP_CONTIG, Arith>(it, ba, smem, mp, layout, &s_flag);
-    else if (it.shape == 11) run_item_tile<6, 16, MAP_INTERLEAVED, Arith>(it, ba, smem, mp, layout, &s_flag);
-    else run_item_engine<Arith>(it, ba, smem, mp, layout, &s_flag);
+    if (it.shape == 0) run_item_tiny<1, Arith, MINB>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 1) run_item_tiny<2, Arith, MINB>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 9) run_item_tile<10, 1, MAP_CONTIG, Arith, MINB>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 8) run_item_tile<9, 2, MAP_CONTIG, Arith, MINB>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 7) run_item_tile<8, 4, MAP_CONTIG, Arith, MINB>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 6) run_item_tile<7, 8, MAP_CONTIG, Arith, MINB>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 11) run_item_tile<6, 16, MAP_INTERLEAVED, Arith, MINB>(it, ba, smem, mp, layout, &s_flag);
+    else run_item_engine<Arith, MINB>(it, ba, smem, mp, layout, &s_flag);
     __syncthreads();  // smem and s_item are reused by the next item
   }
 }
