@@ -70,6 +70,25 @@ struct NttEngine {
   };
   __device__ __forceinline__ static int pad(int l) { return l + (l >> 3); }
 
+  // Stage t of a group of 2^r elements starting at register e0: butterflies
+  // of distance 2^(r-1-t), twiddle T[(gt << t) + u] for the u-th block.
+  template <int r, int t, bool INV>
+  __device__ __forceinline__ static void stage(U128 (&v)[R], int e0, uint32_t gt, const uint4* tw,
+                                               const ModParams& mp) {
+    constexpr int half = 1 << (r - 1 - t);
+#pragma unroll
+    for (int u = 0; u < (1 << t); ++u) {
+      const uint4 tv = __ldg(tw + ((gt << t) + (uint32_t)u));
+      const U128 w = U128{{tv.x, tv.y, tv.z, tv.w}};
+#pragma unroll
+      for (int k = 0; k < half; ++k) {
+        const int j = e0 + ((u << (r - t)) | k);
+        if constexpr (INV) gs_butterfly<Arith>(v[j], v[j + half], w, mp);
+        else butterfly<Arith>(v[j], v[j + half], w, mp);
+      }
+    }
+  }
+
   // One pass of width r (1 <= r <= LOGR) over the thread's GPT = R / 2^r
   // groups: gather (global on the first pass, else shared), r butterfly
   // stages with static register indices, scatter (global on the last pass).
@@ -131,24 +150,34 @@ struct NttEngine {
         }
       }
     }
-    // r stages per group; stage t of the group reads T[(gt << t) + u], u < 2^t
+    // r stages per group; stage t of the group reads T[(gt << t) + u],
+    // u < 2^t.  The inverse runs them in reverse order; with 3 or 4 stages
+    // each of its stages is a separate instantiation (stage()), since the
+    // compiler otherwise keeps v in local memory for the reversed loop.
 #pragma unroll
     for (int i = 0; i < GPT; ++i) {
       const int g = lane + i * tpt;
       const uint32_t gt = (sr.trow << s0) + (uint32_t)(g >> lo);
+      if constexpr (INV && r > 2) {
+        if constexpr (r > 3) stage<r, 3, true>(v, i * G, gt, sr.tw, mp);
+        stage<r, 2, true>(v, i * G, gt, sr.tw, mp);
+        stage<r, 1, true>(v, i * G, gt, sr.tw, mp);
+        stage<r, 0, true>(v, i * G, gt, sr.tw, mp);
+      } else {
 #pragma unroll
-      for (int tt = 0; tt < r; ++tt) {
-        const int t = INV ? r - 1 - tt : tt;
-        const int half = 1 << (r - 1 - t);
+        for (int tt = 0; tt < r; ++tt) {
+          const int t = INV ? r - 1 - tt : tt;
+          const int half = 1 << (r - 1 - t);
 #pragma unroll
-        for (int u = 0; u < (1 << t); ++u) {
-          const uint4 tv = __ldg(sr.tw + ((gt << t) + (uint32_t)u));
-          const U128 w = U128{{tv.x, tv.y, tv.z, tv.w}};
+          for (int u = 0; u < (1 << t); ++u) {
+            const uint4 tv = __ldg(sr.tw + ((gt << t) + (uint32_t)u));
+            const U128 w = U128{{tv.x, tv.y, tv.z, tv.w}};
 #pragma unroll
-          for (int k = 0; k < half; ++k) {
-            const int j = (u << (r - t)) | k;
-            if constexpr (INV) gs_butterfly<Arith>(v[i * G + j], v[i * G + j + half], w, mp);
-            else butterfly<Arith>(v[i * G + j], v[i * G + j + half], w, mp);
+            for (int k = 0; k < half; ++k) {
+              const int j = (u << (r - t)) | k;
+              if constexpr (INV) gs_butterfly<Arith>(v[i * G + j], v[i * G + j + half], w, mp);
+              else butterfly<Arith>(v[i * G + j], v[i * G + j + half], w, mp);
+            }
           }
         }
       }
