@@ -69,8 +69,9 @@ typedef struct bntt_modulus {
  * AUTO: a pseudo-Mersenne multiply when q = 2^124 - k (k < 2^28) and
  *       mu = floor(2^251/q) -- both reference moduli and the NTT-friendly
  *       primes of bntt_ntt_prime -- for which the
- *       reference's Barrett reduction provably returns a*b mod q exactly;
- *       otherwise the replica below.
+ *       reference's Barrett reduction provably returns a*b mod q exactly
+ *       for operands below 2^124 (every residue); otherwise the replica
+ *       below.  Inputs at or above 2^124 need REFERENCE.
  * REFERENCE: a word-for-word replica of mulmod128 (src/ntt_scalar.c:173-199),
  *       identical to the reference for any 128-bit operands. */
 #define BNTT_ARITH_AUTO 0
