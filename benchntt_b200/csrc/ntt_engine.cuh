@@ -182,6 +182,18 @@ struct NttEngine {
         }
       }
     }
+    // the inverse's N^-1 (EPI_SCALE_AT): the upper half of each group holds
+    // y outputs of the last stage, whose table entry carries it already
+    if constexpr ((EPI & EPI_SCALE_AT) != 0) {
+      if (last && ep && sr.valid) {
+        const uint4 f = __ldg(ep->scale_at);
+        const U128 fs = U128{{f.x, f.y, f.z, f.w}};
+#pragma unroll
+        for (int i = 0; i < GPT; ++i)
+#pragma unroll
+          for (int j = 0; j < (INV ? G / 2 : G); ++j) v[i * G + j] = Arith::mul(v[i * G + j], fs, mp);
+      }
+    }
     // scatter
 #pragma unroll
     for (int i = 0; i < GPT; ++i) {
@@ -198,12 +210,6 @@ struct NttEngine {
                 const bool scaled = !INV || j < G / 2;
                 if constexpr ((EPI & EPI_SCALE) != 0) {
                   if (ep->has_scale && scaled) v[i * G + j] = Arith::mul(v[i * G + j], ep->scale, mp);
-                }
-                if constexpr ((EPI & EPI_SCALE_AT) != 0) {  // loaded here: nothing held across the pass
-                  if (scaled) {
-                    const uint4 f = __ldg(ep->scale_at);
-                    v[i * G + j] = Arith::mul(v[i * G + j], U128{{f.x, f.y, f.z, f.w}}, mp);
-                  }
                 }
                 if ((EPI & EPI_MUL) != 0 && ep->mul.b) {
                   const uint4 bv = __ldg(ep->mul.b + ((uint64_t)(yp - ep->mul.ybase) & ep->mul.bmask));
