@@ -1,7 +1,8 @@
 // batch_kinv.cu -- the persistent batch kernel for inverse transforms
 // (bntt_batch_run_inverse_dev).  Same work queue and items as k_batch; each
-// item runs the inverse network (ntt_engine.cuh in inverse mode, stages last
-// to first with the plans' inverse tables), the passes of a large job run
+// item runs the inverse network (the compile-time tile's run_inv for the
+// shapes k_batch runs on tiles, else ntt_engine.cuh in inverse mode; stages
+// last to first with the plans' inverse tables), the passes of a large job run
 // from the last to the first, and whatever finishes a transform -- a small
 // tile, or pass 0 of a large job -- multiplies by N^-1 as it stores, read
 // from entry 0 of the job's inverse table (no stage uses that entry).
@@ -58,6 +59,22 @@ __device__ __noinline__ void run_item_engine_inv(const WorkItem& it, const Batch
   item_publish(it, ba);
 }
 
+// The shapes that carry most work on the compile-time tile, as in k_batch:
+// contiguous 2^7..2^10 and the interleaved 2^6 passes of large jobs.
+template <int M, int TPC, int MAP>
+__device__ __noinline__ void run_item_tile_inv(const WorkItem& it, const BatchArgs& ba, uint4* smem,
+                                               const ModParams& mp, int layout, int* s_flag) {
+  using T = NttTile<M, kBatchLogR, TPC, MAP, ArithFast>;
+  static_assert(T::THREADS == kBatchThreads, "tile shape");
+  const int sub = T::sub_of(threadIdx.x), lane = T::lane_of(threadIdx.x);
+  SubRef sr;
+  if (!item_subref<true>(it, ba, M, sub, s_flag, &sr)) return;
+  const bool finishes = it.kind == ITEM_SMALL || it.pass == 0;
+  const uint4* scale_at = !finishes ? nullptr : it.kind == ITEM_SMALL ? sr.tw : ba.jobs[it.a].tw;
+  T::template run_inv<LD_CG>(sr, sub, lane, smem, mp, layout, scale_at);
+  item_publish(it, ba);
+}
+
 template <int MINB>
 __global__ void __launch_bounds__(kBatchThreads, MINB)
     k_batch_inv(BatchArgs ba, ModParams mp, int layout) {
@@ -72,6 +89,11 @@ __global__ void __launch_bounds__(kBatchThreads, MINB)
     const WorkItem it = ba.items[i];
     if (it.shape == 0) run_item_tiny_inv<1>(it, ba, mp, layout, &s_flag);
     else if (it.shape == 1) run_item_tiny_inv<2>(it, ba, mp, layout, &s_flag);
+    else if (it.shape == 9) run_item_tile_inv<10, 1, MAP_CONTIG>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 8) run_item_tile_inv<9, 2, MAP_CONTIG>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 7) run_item_tile_inv<8, 4, MAP_CONTIG>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 6) run_item_tile_inv<7, 8, MAP_CONTIG>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 11) run_item_tile_inv<6, 16, MAP_INTERLEAVED>(it, ba, smem, mp, layout, &s_flag);
     else run_item_engine_inv(it, ba, smem, mp, layout, &s_flag);
     __syncthreads();  // smem and s_item are reused by the next item
   }

@@ -237,6 +237,115 @@ struct NttTile {
       pass<P + 1, LDP, SRC>(v, sr, sub, lane, smem, mp, layout, mb);
     }
   }
+
+  // The inverse network of the same passes: the last pass first, each pass's
+  // stages in reverse order as Gentleman-Sande butterflies on the inverse
+  // table (gs_butterfly).  The store that finishes the transform (pass 0)
+  // multiplies the lower half of each group -- the x outputs of stage 0 --
+  // by *scale_at (N^-1) when scale_at is not null; the upper half gets N^-1
+  // through the inverse table's entry 1.  Fast moduli only.
+  template <int LDP>
+  __device__ __forceinline__ static void run_inv(const SubRef& sr, int sub, int lane, uint4* smem,
+                                                 const ModParams& mp, int layout,
+                                                 const uint4* scale_at) {
+    U128 v[R];
+    pass_inv<NPASS - 1, LDP>(v, sr, sub, lane, smem, mp, layout, scale_at);
+  }
+
+  // stage t of a group of 2^r registers from e0, inverse butterflies
+  template <int r, int t>
+  __device__ __forceinline__ static void stage_inv(U128 (&v)[R], int e0, uint32_t gt,
+                                                   const uint4* tw, const ModParams& mp) {
+    constexpr int half = 1 << (r - 1 - t);
+#pragma unroll
+    for (int u = 0; u < (1 << t); ++u) {
+      const uint4 tv = __ldg(tw + ((gt << t) + (uint32_t)u));
+      const U128 w = U128{{tv.x, tv.y, tv.z, tv.w}};
+#pragma unroll
+      for (int k = 0; k < half; ++k) {
+        const int j = e0 + ((u << (r - t)) | k);
+        gs_butterfly<Arith>(v[j], v[j + half], w, mp);
+      }
+    }
+  }
+
+  template <int P, int LDP>
+  __device__ __forceinline__ static void pass_inv(U128 (&v)[R], const SubRef& sr, int sub, int lane,
+                                                  uint4* smem, const ModParams& mp, int layout,
+                                                  const uint4* scale_at) {
+    constexpr int r = bits(P);
+    constexpr int s0 = start(P);
+    constexpr int lo = M - s0 - r;
+    constexpr int G = 1 << r;
+    constexpr int GPT = R / G;
+    static_assert(GPT >= 1 && r <= 4, "pass shape");
+
+    // ---- gather: the inverse reads its input in the last pass's order
+#pragma unroll
+    for (int i = 0; i < GPT; ++i) {
+      const int g = lane + i * TPT;
+      const int base = (g & ((1 << lo) - 1)) | ((g >> lo) << (lo + r));
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const int idx = base | (j << lo);
+        if constexpr (P == NPASS - 1) {
+          if (sr.valid) {
+            v[i * G + j] = from_mem(ld_data<LDP>(sr.x + ((size_t)idx << sr.lshift)), layout);
+          } else {
+#pragma unroll
+            for (int w = 0; w < 4; ++w) v[i * G + j].w[w] = 0u;
+          }
+        } else {
+          const uint4 t = smem[slot(sub, idx)];
+          v[i * G + j] = U128{{t.x, t.y, t.z, t.w}};
+        }
+      }
+    }
+
+    // ---- r stages on each group, the last first
+#pragma unroll
+    for (int i = 0; i < GPT; ++i) {
+      const int g = lane + i * TPT;
+      const uint32_t gt = (sr.trow << s0) + (uint32_t)(g >> lo);
+      if constexpr (r > 3) stage_inv<r, 3>(v, i * G, gt, sr.tw, mp);
+      if constexpr (r > 2) stage_inv<r, 2>(v, i * G, gt, sr.tw, mp);
+      if constexpr (r > 1) stage_inv<r, 1>(v, i * G, gt, sr.tw, mp);
+      stage_inv<r, 0>(v, i * G, gt, sr.tw, mp);
+    }
+
+    // ---- N^-1 on the finishing store
+    if constexpr (P == 0) {
+      if (scale_at && sr.valid) {
+        const uint4 f = __ldg(scale_at);
+        const U128 fs = U128{{f.x, f.y, f.z, f.w}};
+#pragma unroll
+        for (int i = 0; i < GPT; ++i)
+#pragma unroll
+          for (int j = 0; j < G / 2; ++j) v[i * G + j] = Arith::mul(v[i * G + j], fs, mp);
+      }
+    }
+
+    // ---- scatter
+#pragma unroll
+    for (int i = 0; i < GPT; ++i) {
+      const int g = lane + i * TPT;
+      const int base = (g & ((1 << lo) - 1)) | ((g >> lo) << (lo + r));
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const int idx = base | (j << lo);
+        if constexpr (P == 0) {
+          if (sr.valid) sr.y[(size_t)idx << sr.lshift] = to_mem(v[i * G + j], layout);
+        } else {
+          const U128& e = v[i * G + j];
+          smem[slot(sub, idx)] = make_uint4(e.w[0], e.w[1], e.w[2], e.w[3]);
+        }
+      }
+    }
+    if constexpr (P > 0) {
+      sync();
+      pass_inv<P - 1, LDP>(v, sr, sub, lane, smem, mp, layout, scale_at);
+    }
+  }
 };
 
 // Geometry of one launch over sub-transforms (see the header comment).
