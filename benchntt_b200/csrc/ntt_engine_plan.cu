@@ -16,9 +16,11 @@
 // no such code); results are canonical residues in [0, q).  The fast
 // pseudo-Mersenne multiply is required (q = 2^124 - k, k < 2^28).
 //
-// Kernels: the runtime-size tile engine (ntt_engine.cuh) in inverse mode,
-// one launch per HBM pass in reverse pass order (the pass over the low index
-// bits first), and a one-thread-per-transform kernel for N = 2 and 4.  The
+// Kernels: the compile-time tile in inverse mode for N = 2^3..2^10 (one
+// launch), the runtime-size tile engine (ntt_engine.cuh) in inverse mode
+// above 2^10, one launch per HBM pass in reverse pass order (the pass over the
+// low index bits first), and a one-thread-per-transform kernel for N = 2 and
+// 4.  The
 // same engine kernel in forward mode runs the plans' forward transforms
 // above 2^10 points (engine_forward_on): passes of at most 8 stages keep the
 // strided passes coalesced.
@@ -78,6 +80,55 @@ __global__ void __launch_bounds__(256)
   }
   // the second half already carries N^-1 through table entry 1
   for (int i = 0; i < N; ++i) x[t * N + i] = to_mem(i < N / 2 ? ArithFast::mul(v[i], scale, mp) : v[i], layout);
+}
+
+// 2^3..2^10 points: the compile-time tile in inverse mode (NttTile::run_inv,
+// 4 elements per thread, 256-thread CTAs of 256 / 2^(M-2) transforms, 4
+// resident per SM), persistent over the tiles like the forward k_ntt_sub.
+// N^-1 comes from entry 0 of the inverse table.
+template <int M>
+__global__ void __launch_bounds__(256, 4)
+    k_ntt_sub_inv(SubGeom g, ModParams mp, int layout) {
+  constexpr int TPC = 256 >> (M - 2);
+  using T = NttTile<M, 2, TPC, MAP_CONTIG, ArithFast>;
+  static_assert(T::THREADS == 256, "tile shape");
+  extern __shared__ uint4 smem[];
+  const int sub = T::sub_of(threadIdx.x), lane = T::lane_of(threadIdx.x);
+  const uint64_t ntiles = (g.nsub + TPC - 1) / TPC;
+  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const SubRef sr = make_subref(g, tile * TPC + (uint64_t)sub);
+    T::template run_inv<LD_NC>(sr, sub, lane, smem, mp, layout, g.tw);
+    T::sync();  // smem is reused by the next tile
+  }
+}
+
+template <int M>
+int launch_sub_inv(bntt_plan* p, void* x, const void* y, size_t batch, cudaStream_t s) {
+  constexpr int TPC = 256 >> (M - 2);
+  using T = NttTile<M, 2, TPC, MAP_CONTIG, ArithFast>;
+  constexpr size_t smem = (size_t)T::SMEM_SLOTS * 16;
+  static std::atomic<int> cached{0};  // resident CTAs per SM; relaxed: same value from any thread
+  int bps = cached.load(std::memory_order_relaxed);
+  if (!bps) {
+    BNTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, (const void*)k_ntt_sub_inv<M>, 256, smem));
+    bps = std::max(1, bps);
+    cached.store(bps, std::memory_order_relaxed);
+  }
+  SubGeom g;
+  g.x = static_cast<const uint4*>(y);
+  g.y = static_cast<uint4*>(x);
+  g.tw = static_cast<const uint4*>(p->tw_inv);
+  g.n = M;
+  g.s0 = 0;
+  g.m = M;
+  g.l = 0;
+  g.nsub = batch;
+  const uint64_t ntiles = (batch + TPC - 1) / TPC;
+  const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)bps * p->ctx->sms);
+  k_ntt_sub_inv<M><<<grid, 256, smem, s>>>(g, p->mp, p->layout);
+  BNTT_CK(cudaGetLastError());
+  p->ctx->launches++;
+  return BNTT_OK;
 }
 
 template <bool INV>
@@ -207,6 +258,17 @@ int inverse_on(bntt_plan* p, void* x, const void* y, size_t batch, cudaStream_t 
     BNTT_CK(cudaGetLastError());
     p->ctx->launches++;
     return BNTT_OK;
+  }
+  switch (n) {
+    case 3: return launch_sub_inv<3>(p, x, y, batch, s);
+    case 4: return launch_sub_inv<4>(p, x, y, batch, s);
+    case 5: return launch_sub_inv<5>(p, x, y, batch, s);
+    case 6: return launch_sub_inv<6>(p, x, y, batch, s);
+    case 7: return launch_sub_inv<7>(p, x, y, batch, s);
+    case 8: return launch_sub_inv<8>(p, x, y, batch, s);
+    case 9: return launch_sub_inv<9>(p, x, y, batch, s);
+    case 10: return launch_sub_inv<10>(p, x, y, batch, s);
+    default: break;
   }
   Epilogue ep;
   ep.scale = p->ninv;

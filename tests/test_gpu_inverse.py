@@ -48,8 +48,8 @@ def forward(ctx, plan, x):
     return dev_call(ctx, plan, bn.lib().bntt_ntt_forward_dev, x)
 
 
-@pytest.mark.parametrize("logn,batch", [(1, 9), (2, 5), (3, 300), (4, 33), (6, 40), (9, 8),
-                                        (10, 16), (11, 4), (12, 2), (13, 1)])
+@pytest.mark.parametrize("logn,batch", [(1, 9), (2, 5), (3, 300), (4, 33), (5, 70), (6, 40), (7, 20),
+                                        (8, 9), (9, 8), (10, 16), (10, 1500), (11, 4), (12, 2), (13, 1)])
 def test_inverse_matches_oracle(ctx, logn, batch):
     n = 1 << logn
     t = C.uniform_pairs(2000 + logn, n, C.Q_NTT)
