@@ -139,6 +139,24 @@ struct NttTile {
     else __syncthreads();
   }
 
+  // Lowest local bit pass p touches.
+  __host__ __device__ static constexpr int low(int p) { return M - start(p) - bits(p); }
+  // Passes a and b exchange within each warp when both hold one group per
+  // thread (r = LOGR) of a contiguous tile and both start at local bit 5 or
+  // below: a warp's 32 consecutive groups then cover the indices whose bits
+  // from 5 + LOGR up equal the warp's number, in both passes, so each warp
+  // reads back only slots it wrote itself (the slot swizzle keeps indices in
+  // their 8-aligned block).
+  __host__ __device__ static constexpr bool warp_exchange(int a, int b) {
+    return WARP_LOCAL || (MAP == MAP_CONTIG && bits(a) == LOGR && bits(b) == LOGR && low(a) <= 5 &&
+                          low(b) <= 5);
+  }
+  template <int A, int B>
+  __device__ __forceinline__ static void sync_between() {
+    if constexpr (warp_exchange(A, B)) __syncwarp();
+    else __syncthreads();
+  }
+
   // Runs the whole sub-transform.  Every thread of the tile must call it
   // (it synchronises); threads whose sub-transform is not valid compute on
   // zeros and store nothing.
@@ -233,7 +251,7 @@ struct NttTile {
       }
     }
     if constexpr (P + 1 < NPASS) {
-      sync();
+      sync_between<P, P + 1>();
       pass<P + 1, LDP, SRC>(v, sr, sub, lane, smem, mp, layout, mb);
     }
   }
@@ -342,7 +360,7 @@ struct NttTile {
       }
     }
     if constexpr (P > 0) {
-      sync();
+      sync_between<P, P - 1>();
       pass_inv<P - 1, LDP>(v, sr, sub, lane, smem, mp, layout, scale_at);
     }
   }

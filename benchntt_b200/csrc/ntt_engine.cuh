@@ -270,7 +270,13 @@ struct NttEngine {
       else if (LOGR != 3)
         pass<1, LDP, INV, EPI>(v, sr, s0, lo, lane, tpt, first, last, lay, smem, mp, layout, ep);
       if (!last) {
-        if (warp_local) __syncwarp();
+        // the next pass exchanges within each warp when both hold one group
+        // per thread of a contiguous tile and start at local bit 5 or below
+        // (NttTile::warp_exchange); M and the mapping are the same for the
+        // whole CTA, so every thread takes the same branch
+        const int pn = INV ? p - 1 : p + 1;
+        const int rn = ps.bits(pn), lon = M - ps.start(pn) - rn;
+        if (warp_local || (contig && r == LOGR && rn == LOGR && lo <= 5 && lon <= 5)) __syncwarp();
         else __syncthreads();
       }
     }
