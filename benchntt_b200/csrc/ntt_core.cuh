@@ -139,6 +139,18 @@ struct NttTile {
     else __syncthreads();
   }
 
+  // slot(sub, base | c) from sb = slot(sub, base) when base and c share no
+  // bit and c is a constant (c = j << lo in a pass): the swizzle
+  // x ^ ((x >> 3) & 7) is linear over XOR, so a contiguous tile's slot is
+  // sb ^ swizzle(c); without swizzle, and for interleaved tiles, the parts
+  // add.  One operation per element, with the constant folded.
+  __host__ __device__ static constexpr int swz(int c) { return (M >= 3) ? (c ^ ((c >> 3) & 7)) : c; }
+  __device__ __forceinline__ static int slot_at(int sb, int c) {
+    if constexpr (MAP == MAP_INTERLEAVED) return sb + c * TPC;
+    else if constexpr (M >= 3) return sb ^ swz(c);
+    else return sb + c;
+  }
+
   // Lowest local bit pass p touches.
   __host__ __device__ static constexpr int low(int p) { return M - start(p) - bits(p); }
   // Passes a and b exchange within each warp when both hold one group per
@@ -184,11 +196,12 @@ struct NttTile {
     for (int i = 0; i < GPT; ++i) {
       const int g = lane + i * TPT;
       const int base = (g & ((1 << lo) - 1)) | ((g >> lo) << (lo + r));
+      const int sb = slot(sub, base);
 #pragma unroll
       for (int j = 0; j < G; ++j) {
         const int idx = base | (j << lo);
         if constexpr (P == 0 && (SRC & SRC_STAGED) != 0) {
-          v[i * G + j] = from_mem(smem[slot(sub, idx)], layout);  // staged in memory order
+          v[i * G + j] = from_mem(smem[slot_at(sb, j << lo)], layout);  // staged in memory order
         } else if constexpr (P == 0) {
           if (sr.valid) {
             v[i * G + j] = from_mem(ld_data<LDP>(sr.x + ((size_t)idx << sr.lshift)), layout);
@@ -197,7 +210,7 @@ struct NttTile {
             for (int w = 0; w < 4; ++w) v[i * G + j].w[w] = 0u;
           }
         } else {
-          const uint4 t = smem[slot(sub, idx)];
+          const uint4 t = smem[slot_at(sb, j << lo)];
           v[i * G + j] = U128{{t.x, t.y, t.z, t.w}};
         }
       }
@@ -231,6 +244,7 @@ struct NttTile {
     for (int i = 0; i < GPT; ++i) {
       const int g = lane + i * TPT;
       const int base = (g & ((1 << lo) - 1)) | ((g >> lo) << (lo + r));
+      const int sb = slot(sub, base);
 #pragma unroll
       for (int j = 0; j < G; ++j) {
         const int idx = base | (j << lo);
@@ -246,7 +260,7 @@ struct NttTile {
           }
         } else {
           const U128& e = v[i * G + j];
-          smem[slot(sub, idx)] = make_uint4(e.w[0], e.w[1], e.w[2], e.w[3]);
+          smem[slot_at(sb, j << lo)] = make_uint4(e.w[0], e.w[1], e.w[2], e.w[3]);
         }
       }
     }
@@ -303,6 +317,7 @@ struct NttTile {
     for (int i = 0; i < GPT; ++i) {
       const int g = lane + i * TPT;
       const int base = (g & ((1 << lo) - 1)) | ((g >> lo) << (lo + r));
+      const int sb = slot(sub, base);
 #pragma unroll
       for (int j = 0; j < G; ++j) {
         const int idx = base | (j << lo);
@@ -314,7 +329,7 @@ struct NttTile {
             for (int w = 0; w < 4; ++w) v[i * G + j].w[w] = 0u;
           }
         } else {
-          const uint4 t = smem[slot(sub, idx)];
+          const uint4 t = smem[slot_at(sb, j << lo)];
           v[i * G + j] = U128{{t.x, t.y, t.z, t.w}};
         }
       }
@@ -348,6 +363,7 @@ struct NttTile {
     for (int i = 0; i < GPT; ++i) {
       const int g = lane + i * TPT;
       const int base = (g & ((1 << lo) - 1)) | ((g >> lo) << (lo + r));
+      const int sb = slot(sub, base);
 #pragma unroll
       for (int j = 0; j < G; ++j) {
         const int idx = base | (j << lo);
@@ -355,7 +371,7 @@ struct NttTile {
           if (sr.valid) sr.y[(size_t)idx << sr.lshift] = to_mem(v[i * G + j], layout);
         } else {
           const U128& e = v[i * G + j];
-          smem[slot(sub, idx)] = make_uint4(e.w[0], e.w[1], e.w[2], e.w[3]);
+          smem[slot_at(sb, j << lo)] = make_uint4(e.w[0], e.w[1], e.w[2], e.w[3]);
         }
       }
     }
