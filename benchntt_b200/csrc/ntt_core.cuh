@@ -190,6 +190,8 @@ struct NttTile {
     constexpr int G = 1 << r;             // elements per group
     constexpr int GPT = R / G;            // groups per thread
     static_assert(GPT >= 1, "pass wider than the register tile");
+    // element j of a group in HBM: the group's first element plus j * gstep
+    const size_t gstep = (size_t)1 << (lo + sr.lshift);
 
     // ---- gather
 #pragma unroll
@@ -199,12 +201,11 @@ struct NttTile {
       const int sb = slot(sub, base);
 #pragma unroll
       for (int j = 0; j < G; ++j) {
-        const int idx = base | (j << lo);
         if constexpr (P == 0 && (SRC & SRC_STAGED) != 0) {
           v[i * G + j] = from_mem(smem[slot_at(sb, j << lo)], layout);  // staged in memory order
         } else if constexpr (P == 0) {
           if (sr.valid) {
-            v[i * G + j] = from_mem(ld_data<LDP>(sr.x + ((size_t)idx << sr.lshift)), layout);
+            v[i * G + j] = from_mem(ld_data<LDP>(sr.x + ((size_t)base << sr.lshift) + (size_t)j * gstep), layout);
           } else {
 #pragma unroll
             for (int w = 0; w < 4; ++w) v[i * G + j].w[w] = 0u;
@@ -227,8 +228,8 @@ struct NttTile {
 #pragma unroll
         for (int u = 0; u < (1 << t); ++u) {
           // tables are stored in limb order (LAYOUT_U128) by the plan
-          const uint4 tv = (SRC & TW_SHARED) != 0 ? lds128(sr.tw + ((gt << t) + (uint32_t)u))
-                                                  : __ldg(sr.tw + ((gt << t) + (uint32_t)u));
+          const uint4* twt = sr.tw + (gt << t);  // u as an immediate offset
+          const uint4 tv = (SRC & TW_SHARED) != 0 ? lds128(twt + u) : __ldg(twt + u);
           const U128 w = U128{{tv.x, tv.y, tv.z, tv.w}};
 #pragma unroll
           for (int k = 0; k < half; ++k) {
@@ -247,10 +248,9 @@ struct NttTile {
       const int sb = slot(sub, base);
 #pragma unroll
       for (int j = 0; j < G; ++j) {
-        const int idx = base | (j << lo);
         if constexpr (P == NPASS - 1) {
           if (sr.valid) {
-            uint4* yp = sr.y + ((size_t)idx << sr.lshift);
+            uint4* yp = sr.y + ((size_t)base << sr.lshift) + (size_t)j * gstep;
             U128 o = v[i * G + j];
             if (mb.b) {
               const uint4 bv = __ldg(mb.b + ((uint64_t)(yp - mb.ybase) & mb.bmask));
@@ -291,7 +291,7 @@ struct NttTile {
     constexpr int half = 1 << (r - 1 - t);
 #pragma unroll
     for (int u = 0; u < (1 << t); ++u) {
-      const uint4 tv = __ldg(tw + ((gt << t) + (uint32_t)u));
+      const uint4 tv = __ldg(tw + (gt << t) + u);
       const U128 w = U128{{tv.x, tv.y, tv.z, tv.w}};
 #pragma unroll
       for (int k = 0; k < half; ++k) {
@@ -311,6 +311,7 @@ struct NttTile {
     constexpr int G = 1 << r;
     constexpr int GPT = R / G;
     static_assert(GPT >= 1 && r <= 4, "pass shape");
+    const size_t gstep = (size_t)1 << (lo + sr.lshift);  // HBM distance of j and j + 1
 
     // ---- gather: the inverse reads its input in the last pass's order
 #pragma unroll
@@ -320,10 +321,9 @@ struct NttTile {
       const int sb = slot(sub, base);
 #pragma unroll
       for (int j = 0; j < G; ++j) {
-        const int idx = base | (j << lo);
         if constexpr (P == NPASS - 1) {
           if (sr.valid) {
-            v[i * G + j] = from_mem(ld_data<LDP>(sr.x + ((size_t)idx << sr.lshift)), layout);
+            v[i * G + j] = from_mem(ld_data<LDP>(sr.x + ((size_t)base << sr.lshift) + (size_t)j * gstep), layout);
           } else {
 #pragma unroll
             for (int w = 0; w < 4; ++w) v[i * G + j].w[w] = 0u;
@@ -366,9 +366,8 @@ struct NttTile {
       const int sb = slot(sub, base);
 #pragma unroll
       for (int j = 0; j < G; ++j) {
-        const int idx = base | (j << lo);
         if constexpr (P == 0) {
-          if (sr.valid) sr.y[(size_t)idx << sr.lshift] = to_mem(v[i * G + j], layout);
+          if (sr.valid) sr.y[((size_t)base << sr.lshift) + (size_t)j * gstep] = to_mem(v[i * G + j], layout);
         } else {
           const U128& e = v[i * G + j];
           smem[slot_at(sb, j << lo)] = make_uint4(e.w[0], e.w[1], e.w[2], e.w[3]);

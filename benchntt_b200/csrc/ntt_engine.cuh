@@ -78,7 +78,7 @@ struct NttEngine {
     constexpr int half = 1 << (r - 1 - t);
 #pragma unroll
     for (int u = 0; u < (1 << t); ++u) {
-      const uint4 tv = __ldg(tw + ((gt << t) + (uint32_t)u));
+      const uint4 tv = __ldg(tw + (gt << t) + u);
       const U128 w = U128{{tv.x, tv.y, tv.z, tv.w}};
 #pragma unroll
       for (int k = 0; k < half; ++k) {
@@ -170,7 +170,7 @@ struct NttEngine {
           const int half = 1 << (r - 1 - t);
 #pragma unroll
           for (int u = 0; u < (1 << t); ++u) {
-            const uint4 tv = __ldg(sr.tw + ((gt << t) + (uint32_t)u));
+            const uint4 tv = __ldg(sr.tw + (gt << t) + u);
             const U128 w = U128{{tv.x, tv.y, tv.z, tv.w}};
 #pragma unroll
             for (int k = 0; k < half; ++k) {
