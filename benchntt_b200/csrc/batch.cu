@@ -13,7 +13,7 @@
 
 namespace bntt {
 
-const void* batch_kernel_fast_minb(int minb);
+const void* batch_kernel_fast_minb(int minb, int layout);
 const void* batch_kernel_ref();
 
 // Resident CTAs per SM the fast batch kernel is compiled for (2 to 5,
@@ -110,7 +110,9 @@ void free_schedule(bntt_ctx* c, Schedule& s) {
   s.d_ctl_cap = 0;
 }
 
-const void* batch_kernel(bool fast) { return fast ? batch_kernel_fast_minb(g_batch_minb) : batch_kernel_ref(); }
+const void* batch_kernel(bool fast, int layout) {
+  return fast ? batch_kernel_fast_minb(g_batch_minb, layout) : batch_kernel_ref();
+}
 
 constexpr int kMaxLog2n = 24;  // plans hold 2^1..2^24 points
 
@@ -437,7 +439,7 @@ static int upload(bntt_batch* b, Schedule& sc, cudaStream_t stream, bool inverse
   sc.sticky_err = sticky_err;
   sc.grid = 0;
   if (sc.items.empty()) return BNTT_OK;
-  const void* fn = inverse ? batch_kernel_inverse() : batch_kernel(b->fast);
+  const void* fn = inverse ? batch_kernel_inverse(b->layout) : batch_kernel(b->fast, b->layout);
   size_t smem = 0;
   bool used[kNumShapes] = {};
   for (const WorkItem& w : sc.items) used[w.shape] = true;
@@ -469,7 +471,7 @@ static cudaError_t enqueue_run(bntt_batch* b, Schedule& sc, cudaStream_t stream)
     if (e == cudaSuccess && cb > 8) e = cudaMemsetAsync(static_cast<char*>(sc.d_ctl) + 8, 0, cb - 8, stream);
   }
   if (e != cudaSuccess) return e;
-  const void* fn = sc.inverse ? batch_kernel_inverse() : batch_kernel(b->fast);
+  const void* fn = sc.inverse ? batch_kernel_inverse(b->layout) : batch_kernel(b->fast, b->layout);
   BatchArgs ba = sc.args;
   ModParams mp = b->mp;
   int layout = b->layout;
@@ -963,7 +965,7 @@ extern "C" int bntt_batch_run_dev_noalloc(bntt_batch* b, const bntt_job* jobs, s
   if (ob) BNTT_CK(cudaMemcpyAsync(s + o_or, sc.order.data(), ob, cudaMemcpyHostToDevice, st));
   if (jb) BNTT_CK(cudaMemcpyAsync(s + o_jb, sc.djobs.data(), jb, cudaMemcpyHostToDevice, st));
   if (sc.items.empty()) return BNTT_OK;
-  const void* fn = batch_kernel(b->fast);
+  const void* fn = batch_kernel(b->fast, b->layout);
   size_t smem = 0;
   bool used[kNumShapes] = {};
   for (const WorkItem& w : sc.items) used[w.shape] = true;

@@ -108,8 +108,8 @@ namespace bntt {
 // device buffer of at least `bytes` (headroom: a quarter more when it grows)
 int grow(bntt_ctx* c, void** p, size_t* cap, size_t bytes, bool headroom = false);
 void free_schedule(bntt_ctx* c, Schedule& s);
-const void* batch_kernel(bool fast);
-const void* batch_kernel_inverse();
+const void* batch_kernel(bool fast, int layout);
+const void* batch_kernel_inverse(int layout);
 // resident CTAs per SM of a batch kernel (cached per device)
 int batch_kernel_bps(const void* fn, int* bps);
 size_t shape_smem(int s);

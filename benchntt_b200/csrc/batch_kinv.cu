@@ -14,9 +14,10 @@ namespace bntt {
 namespace {
 
 // 2^1, 2^2: one thread per transform.
-template <int M>
+template <int M, int LY>
 __device__ __noinline__ void run_item_tiny_inv(const WorkItem& it, const BatchArgs& ba,
-                                               const ModParams& mp, int layout, int* s_flag) {
+                                               const ModParams& mp, int layout_arg, int* s_flag) {
+  const int layout = LY >= 0 ? LY : layout_arg;
   SubRef sr;
   if (!item_subref<true>(it, ba, M, threadIdx.x, s_flag, &sr)) return;
   if (!sr.valid) return;
@@ -41,8 +42,10 @@ __device__ __noinline__ void run_item_tiny_inv(const WorkItem& it, const BatchAr
     sr.y[i] = to_mem(i < N / 2 ? ArithFast::mul(v[i], ninv, mp) : v[i], layout);
 }
 
+template <int LY>
 __device__ __noinline__ void run_item_engine_inv(const WorkItem& it, const BatchArgs& ba, uint4* smem,
-                                                 const ModParams& mp, int layout, int* s_flag) {
+                                                 const ModParams& mp, int layout_arg, int* s_flag) {
+  const int layout = LY >= 0 ? LY : layout_arg;
   using E = NttEngine<kBatchLogR, ArithFast>;
   int m, map;
   shape_of(it.shape, &m, &map);
@@ -61,9 +64,10 @@ __device__ __noinline__ void run_item_engine_inv(const WorkItem& it, const Batch
 
 // The shapes that carry most work on the compile-time tile, as in k_batch:
 // contiguous 2^7..2^10 and the interleaved 2^6 passes of large jobs.
-template <int M, int TPC, int MAP>
+template <int M, int TPC, int MAP, int LY>
 __device__ __noinline__ void run_item_tile_inv(const WorkItem& it, const BatchArgs& ba, uint4* smem,
-                                               const ModParams& mp, int layout, int* s_flag) {
+                                               const ModParams& mp, int layout_arg, int* s_flag) {
+  const int layout = LY >= 0 ? LY : layout_arg;
   using T = NttTile<M, kBatchLogR, TPC, MAP, ArithFast>;
   static_assert(T::THREADS == kBatchThreads, "tile shape");
   const int sub = T::sub_of(threadIdx.x), lane = T::lane_of(threadIdx.x);
@@ -75,7 +79,8 @@ __device__ __noinline__ void run_item_tile_inv(const WorkItem& it, const BatchAr
   item_publish(it, ba);
 }
 
-template <int MINB>
+// LY: the element layout as a constant, as in k_batch.
+template <int MINB, int LY>
 __global__ void __launch_bounds__(kBatchThreads, MINB)
     k_batch_inv(BatchArgs ba, ModParams mp, int layout) {
   extern __shared__ uint4 smem[];
@@ -87,20 +92,23 @@ __global__ void __launch_bounds__(kBatchThreads, MINB)
     const uint32_t i = s_item;
     if (i >= ba.nitems) break;
     const WorkItem it = ba.items[i];
-    if (it.shape == 0) run_item_tiny_inv<1>(it, ba, mp, layout, &s_flag);
-    else if (it.shape == 1) run_item_tiny_inv<2>(it, ba, mp, layout, &s_flag);
-    else if (it.shape == 9) run_item_tile_inv<10, 1, MAP_CONTIG>(it, ba, smem, mp, layout, &s_flag);
-    else if (it.shape == 8) run_item_tile_inv<9, 2, MAP_CONTIG>(it, ba, smem, mp, layout, &s_flag);
-    else if (it.shape == 7) run_item_tile_inv<8, 4, MAP_CONTIG>(it, ba, smem, mp, layout, &s_flag);
-    else if (it.shape == 6) run_item_tile_inv<7, 8, MAP_CONTIG>(it, ba, smem, mp, layout, &s_flag);
-    else if (it.shape == 11) run_item_tile_inv<6, 16, MAP_INTERLEAVED>(it, ba, smem, mp, layout, &s_flag);
-    else run_item_engine_inv(it, ba, smem, mp, layout, &s_flag);
+    if (it.shape == 0) run_item_tiny_inv<1, LY>(it, ba, mp, layout, &s_flag);
+    else if (it.shape == 1) run_item_tiny_inv<2, LY>(it, ba, mp, layout, &s_flag);
+    else if (it.shape == 9) run_item_tile_inv<10, 1, MAP_CONTIG, LY>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 8) run_item_tile_inv<9, 2, MAP_CONTIG, LY>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 7) run_item_tile_inv<8, 4, MAP_CONTIG, LY>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 6) run_item_tile_inv<7, 8, MAP_CONTIG, LY>(it, ba, smem, mp, layout, &s_flag);
+    else if (it.shape == 11) run_item_tile_inv<6, 16, MAP_INTERLEAVED, LY>(it, ba, smem, mp, layout, &s_flag);
+    else run_item_engine_inv<LY>(it, ba, smem, mp, layout, &s_flag);
     __syncthreads();  // smem and s_item are reused by the next item
   }
 }
 
 }  // namespace
 
-const void* batch_kernel_inverse() { return (const void*)&k_batch_inv<4>; }
+const void* batch_kernel_inverse(int layout) {
+  return layout == LAYOUT_HILO ? (const void*)&k_batch_inv<4, LAYOUT_HILO>
+                               : (const void*)&k_batch_inv<4, LAYOUT_U128>;
+}
 
 }  // namespace bntt

@@ -190,7 +190,7 @@ static int launch_slot(bntt_server* s, Slot& slot) {
     memcpy(h + o_jb, sc.djobs.data(), jb);
     char* d = static_cast<char*>(slot.dev);
     BNTT_CK(cudaMemcpyAsync(d, h, need, cudaMemcpyHostToDevice, slot.stream));
-    const void* fn = batch_kernel(s->engine->fast);
+    const void* fn = batch_kernel(s->engine->fast, s->engine->layout);
     size_t smem = 0;
     for (const WorkItem& w : sc.items) smem = std::max(smem, shape_smem(w.shape));
     // occupancy queried once at creation
@@ -329,7 +329,7 @@ int bntt_server_create(bntt_ctx* c, bntt_server** out, bntt_plan* const* plans, 
     return rc;
   }
   s->arena.init(static_cast<char*>(s->arena_mem), s->cfg.hbm_budget);
-  if ((rc = batch_kernel_bps(batch_kernel(s->engine->fast), &s->batch_bps))) {
+  if ((rc = batch_kernel_bps(batch_kernel(s->engine->fast, s->engine->layout), &s->batch_bps))) {
     ctx_free(c, s->arena_mem);
     bntt_batch_destroy(s->engine);
     delete s;
