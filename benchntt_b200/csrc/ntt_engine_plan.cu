@@ -97,7 +97,8 @@ __global__ void __launch_bounds__(256, 4)
   const uint64_t ntiles = (g.nsub + TPC - 1) / TPC;
   for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const SubRef sr = make_subref(g, tile * TPC + (uint64_t)sub);
-    T::template run_inv<LD_NC>(sr, sub, lane, smem, mp, layout, g.tw);
+    if (layout == LAYOUT_HILO) T::template run_inv<LD_NC>(sr, sub, lane, smem, mp, LAYOUT_HILO, g.tw);
+    else T::template run_inv<LD_NC>(sr, sub, lane, smem, mp, LAYOUT_U128, g.tw);
     T::sync();  // smem is reused by the next tile
   }
 }

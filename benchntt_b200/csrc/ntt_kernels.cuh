@@ -19,7 +19,10 @@ __global__ void __launch_bounds__(NttTile<M, LOGR, TPC, MAP, Arith>::THREADS, MI
   const uint64_t ntiles = (g.nsub + TPC - 1) / TPC;
   for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const SubRef sr = make_subref(g, tile * TPC + (uint64_t)sub);
-    T::template run<LD_NC>(sr, sub, lane, smem, mp, layout, MulB{g.b, g.y, g.bmask});
+    // the element layout as a constant in each branch: no word select per
+    // HBM load and store
+    if (layout == LAYOUT_HILO) T::template run<LD_NC>(sr, sub, lane, smem, mp, LAYOUT_HILO, MulB{g.b, g.y, g.bmask});
+    else T::template run<LD_NC>(sr, sub, lane, smem, mp, LAYOUT_U128, MulB{g.b, g.y, g.bmask});
     if constexpr (T::NPASS > 1) T::sync();  // smem is reused by the next tile
   }
 }
@@ -74,8 +77,12 @@ __global__ void __launch_bounds__(NttTile<M, LOGR, TPC, MAP_CONTIG, Arith>::THRE
     __syncthreads();
     SubRef sr = make_subref(g, tile * TPC + (uint64_t)sub);
     sr.tw = tw;
-    T::template run<LD_NC, SRC | SRC_STAGED>(sr, sub, lane, smem + b * TILE, mp, layout,
-                                             MulB{g.b, g.y, g.bmask});
+    if (layout == LAYOUT_HILO)
+      T::template run<LD_NC, SRC | SRC_STAGED>(sr, sub, lane, smem + b * TILE, mp, LAYOUT_HILO,
+                                               MulB{g.b, g.y, g.bmask});
+    else
+      T::template run<LD_NC, SRC | SRC_STAGED>(sr, sub, lane, smem + b * TILE, mp, LAYOUT_U128,
+                                               MulB{g.b, g.y, g.bmask});
     __syncthreads();  // this buffer is refilled by the next iteration's copy
   }
   cp_async_wait<0>();
