@@ -159,6 +159,8 @@ static const std::vector<int>& split_of(int n) {
   return table[n];
 }
 
+std::vector<int> tile_split(int n) { return n >= 11 && n <= kMaxLog2n ? split_of(n) : std::vector<int>{}; }
+
 // The plans' fields, looked up once instead of per job.
 static void plan_fields(const bntt_batch* b, Schedule& sc, bool inverse) {
   const size_t np = b->plans.size();

@@ -86,6 +86,11 @@ std::vector<int> split_passes(int n, int max_m = 10);
 // HBM passes of a 2^n transform (n > 10) on the tile engine (batch kernel,
 // engine plans): fewest passes of <= 8 stages, then fewest engine passes.
 std::vector<int> engine_split(int n);
+// HBM passes of a 2^n transform (11 <= n <= 24) on 4-element tiles, as the
+// persistent kernel splits its large jobs: strided passes of 5..7 stages
+// (2^(10 - m) adjacent columns per tile), then a contiguous pass of up to 10;
+// the fewest passes, then the fewest tile passes.  Empty outside that range.
+std::vector<int> tile_split(int n);
 
 int launch_blas(bntt_ctx* ctx, int op, void* c, const void* a, const void* b, U128 x, size_t len,
                 const ModParams& mp, bool fast, int layout, cudaStream_t stream);

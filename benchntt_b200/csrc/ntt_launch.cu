@@ -179,7 +179,45 @@ int ntt_forward_on(bntt_plan* plan, void* y, const void* x, size_t batch, cudaSt
   // stages (a strided pass then covers >= 8 adjacent columns, 128 B per
   // row); measured 1.5x faster at 2^16 than compiled tiles with 10-stage
   // passes, whose strided passes touch 2 or 4 columns per tile
-  if (n > 10 && arith_fast(plan->ctx, plan->fast)) return engine_forward_on(plan, y, x, batch, s, b, bmask);
+  if (n > 10 && arith_fast(plan->ctx, plan->fast)) {
+    // the persistent kernel's split and tiles when every pass's shape is
+    // compiled, else the engine
+    const std::vector<int> split = tile_split(n);
+    std::vector<const SubKernel*> ks;
+    int s0 = 0;
+    for (int m : split) {
+      const int map = n - s0 - m > 0 ? MAP_INTERLEAVED : MAP_CONTIG;
+      const SubKernel* found = nullptr;
+      for (const SubKernel& k : sub_kernels())
+        if (k.m == m && k.map == map && k.fast == 1 && k.logr == 2 && k.tpc == (256 >> (m - 2)) &&
+            k.minb == 4 && k.src == 0)
+          found = &k;
+      if (!found) break;
+      ks.push_back(found);
+      s0 += m;
+    }
+    if (split.empty() || ks.size() != split.size()) return engine_forward_on(plan, y, x, batch, s, b, bmask);
+    s0 = 0;
+    for (size_t i = 0; i < split.size(); ++i) {
+      const int m = split[i];
+      SubGeom g;
+      g.x = static_cast<const uint4*>(i == 0 ? x : y);
+      g.y = static_cast<uint4*>(y);
+      g.tw = static_cast<const uint4*>(plan->tw);
+      g.n = (uint32_t)n;
+      g.s0 = (uint32_t)s0;
+      g.m = (uint32_t)m;
+      g.l = (uint32_t)(n - s0 - m);
+      g.nsub = (uint64_t)batch << (n - m);
+      if (i + 1 == split.size()) {
+        g.b = static_cast<const uint4*>(b);
+        g.bmask = bmask;
+      }
+      if (int rc = launch_sub(plan->ctx, ks[i], &g, plan->mp, plan->layout, s)) return rc;
+      s0 += m;
+    }
+    return BNTT_OK;
+  }
   int s0 = 0;
   for (size_t i = 0; i < plan->passes.size(); ++i) {
     const int m = plan->passes[i];
