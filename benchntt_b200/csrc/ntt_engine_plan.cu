@@ -16,14 +16,14 @@
 // no such code); results are canonical residues in [0, q).  The fast
 // pseudo-Mersenne multiply is required (q = 2^124 - k, k < 2^28).
 //
-// Kernels: the compile-time tile in inverse mode for N = 2^3..2^10 (one
-// launch), the runtime-size tile engine (ntt_engine.cuh) in inverse mode
-// above 2^10, one launch per HBM pass in reverse pass order (the pass over the
-// low index bits first), and a one-thread-per-transform kernel for N = 2 and
-// 4.  The
-// same engine kernel in forward mode runs the plans' forward transforms
-// above 2^10 points (engine_forward_on): passes of at most 8 stages keep the
-// strided passes coalesced.
+// Kernels: the compile-time tile in inverse mode (k_ntt_tile_inv), one
+// launch for N = 2^3..2^10 and above that one launch per HBM pass of the
+// persistent kernel's split (tile_split), in reverse pass order (the pass
+// over the low index bits first); a one-thread-per-transform kernel for N = 2
+// and 4.  The runtime-size tile engine (ntt_engine.cuh) in inverse mode
+// remains for splits without a tile kernel, and in forward mode for the
+// forward transforms above 2^10 points (engine_forward_on) likewise: passes
+// of at most 8 stages keep the strided passes coalesced.
 #include <algorithm>
 #include <atomic>
 #include <vector>
@@ -82,54 +82,76 @@ __global__ void __launch_bounds__(256)
   for (int i = 0; i < N; ++i) x[t * N + i] = to_mem(i < N / 2 ? ArithFast::mul(v[i], scale, mp) : v[i], layout);
 }
 
-// 2^3..2^10 points: the compile-time tile in inverse mode (NttTile::run_inv,
-// 4 elements per thread, 256-thread CTAs of 256 / 2^(M-2) transforms, 4
-// resident per SM), persistent over the tiles like the forward k_ntt_sub.
-// N^-1 comes from entry 0 of the inverse table.
-template <int M>
+// One HBM pass of the inverse on the compile-time tile (NttTile::run_inv, 4
+// elements per thread, 256-thread CTAs of 256 / 2^(M-2) sub-transforms, 4
+// resident per SM), persistent over the tiles like the forward k_ntt_sub:
+// whole transforms of 2^3..2^10 points (contiguous), or one pass of a larger
+// transform (interleaved for the strided passes).  `finishing` marks the
+// pass that ends the transform (stage 0 inside it), which applies N^-1 from
+// entry 0 of the inverse table.
+template <int M, int MAP>
 __global__ void __launch_bounds__(256, 4)
-    k_ntt_sub_inv(SubGeom g, ModParams mp, int layout) {
+    k_ntt_tile_inv(SubGeom g, ModParams mp, int layout, int finishing) {
   constexpr int TPC = 256 >> (M - 2);
-  using T = NttTile<M, 2, TPC, MAP_CONTIG, ArithFast>;
+  using T = NttTile<M, 2, TPC, MAP, ArithFast>;
   static_assert(T::THREADS == 256, "tile shape");
   extern __shared__ uint4 smem[];
   const int sub = T::sub_of(threadIdx.x), lane = T::lane_of(threadIdx.x);
   const uint64_t ntiles = (g.nsub + TPC - 1) / TPC;
+  const uint4* scale_at = finishing ? g.tw : nullptr;
   for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const SubRef sr = make_subref(g, tile * TPC + (uint64_t)sub);
-    if (layout == LAYOUT_HILO) T::template run_inv<LD_NC>(sr, sub, lane, smem, mp, LAYOUT_HILO, g.tw);
-    else T::template run_inv<LD_NC>(sr, sub, lane, smem, mp, LAYOUT_U128, g.tw);
+    if (layout == LAYOUT_HILO) T::template run_inv<LD_NC>(sr, sub, lane, smem, mp, LAYOUT_HILO, scale_at);
+    else T::template run_inv<LD_NC>(sr, sub, lane, smem, mp, LAYOUT_U128, scale_at);
     T::sync();  // smem is reused by the next tile
   }
 }
 
-template <int M>
-int launch_sub_inv(bntt_plan* p, void* x, const void* y, size_t batch, cudaStream_t s) {
+template <int M, int MAP>
+int launch_tile_inv(bntt_plan* p, const SubGeom& g, int finishing, cudaStream_t s) {
   constexpr int TPC = 256 >> (M - 2);
-  using T = NttTile<M, 2, TPC, MAP_CONTIG, ArithFast>;
+  using T = NttTile<M, 2, TPC, MAP, ArithFast>;
   constexpr size_t smem = (size_t)T::SMEM_SLOTS * 16;
   static std::atomic<int> cached{0};  // resident CTAs per SM; relaxed: same value from any thread
   int bps = cached.load(std::memory_order_relaxed);
   if (!bps) {
-    BNTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, (const void*)k_ntt_sub_inv<M>, 256, smem));
+    BNTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, (const void*)k_ntt_tile_inv<M, MAP>, 256, smem));
     bps = std::max(1, bps);
     cached.store(bps, std::memory_order_relaxed);
   }
-  SubGeom g;
-  g.x = static_cast<const uint4*>(y);
-  g.y = static_cast<uint4*>(x);
-  g.tw = static_cast<const uint4*>(p->tw_inv);
-  g.n = M;
-  g.s0 = 0;
-  g.m = M;
-  g.l = 0;
-  g.nsub = batch;
-  const uint64_t ntiles = (batch + TPC - 1) / TPC;
+  const uint64_t ntiles = (g.nsub + TPC - 1) / TPC;
   const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)bps * p->ctx->sms);
-  k_ntt_sub_inv<M><<<grid, 256, smem, s>>>(g, p->mp, p->layout);
+  k_ntt_tile_inv<M, MAP><<<grid, 256, smem, s>>>(g, p->mp, p->layout, finishing);
   BNTT_CK(cudaGetLastError());
   p->ctx->launches++;
   return BNTT_OK;
+}
+
+// One pass of m stages (a whole transform of 2^3..2^10 points, a strided
+// pass of 5..7 or a contiguous last pass of a larger one); EINVAL for a shape
+// without a tile kernel.
+int tile_inv_pass(bntt_plan* p, const SubGeom& g, int finishing, cudaStream_t s) {
+  if (g.l > 0) {
+    switch (g.m) {
+      case 5: return launch_tile_inv<5, MAP_INTERLEAVED>(p, g, finishing, s);
+      case 6: return launch_tile_inv<6, MAP_INTERLEAVED>(p, g, finishing, s);
+      case 7: return launch_tile_inv<7, MAP_INTERLEAVED>(p, g, finishing, s);
+      default: break;
+    }
+  } else {
+    switch (g.m) {
+      case 3: return launch_tile_inv<3, MAP_CONTIG>(p, g, finishing, s);
+      case 4: return launch_tile_inv<4, MAP_CONTIG>(p, g, finishing, s);
+      case 5: return launch_tile_inv<5, MAP_CONTIG>(p, g, finishing, s);
+      case 6: return launch_tile_inv<6, MAP_CONTIG>(p, g, finishing, s);
+      case 7: return launch_tile_inv<7, MAP_CONTIG>(p, g, finishing, s);
+      case 8: return launch_tile_inv<8, MAP_CONTIG>(p, g, finishing, s);
+      case 9: return launch_tile_inv<9, MAP_CONTIG>(p, g, finishing, s);
+      case 10: return launch_tile_inv<10, MAP_CONTIG>(p, g, finishing, s);
+      default: break;
+    }
+  }
+  return set_error(BNTT_EINVAL, "no inverse tile for a pass of %u stages", g.m);
 }
 
 template <bool INV>
@@ -260,16 +282,28 @@ int inverse_on(bntt_plan* p, void* x, const void* y, size_t batch, cudaStream_t 
     p->ctx->launches++;
     return BNTT_OK;
   }
-  switch (n) {
-    case 3: return launch_sub_inv<3>(p, x, y, batch, s);
-    case 4: return launch_sub_inv<4>(p, x, y, batch, s);
-    case 5: return launch_sub_inv<5>(p, x, y, batch, s);
-    case 6: return launch_sub_inv<6>(p, x, y, batch, s);
-    case 7: return launch_sub_inv<7>(p, x, y, batch, s);
-    case 8: return launch_sub_inv<8>(p, x, y, batch, s);
-    case 9: return launch_sub_inv<9>(p, x, y, batch, s);
-    case 10: return launch_sub_inv<10>(p, x, y, batch, s);
-    default: break;
+  // up to 2^10 points one tile pass; above, the persistent kernel's split
+  // (strided passes of 5..7 stages, then a contiguous one), run last pass
+  // first, the first run reading y and every run writing x
+  const std::vector<int> split = n <= 10 ? std::vector<int>{n} : tile_split(n);
+  if (!split.empty()) {
+    const int np = (int)split.size();
+    std::vector<int> starts(np, 0);
+    for (int i = 1; i < np; ++i) starts[i] = starts[i - 1] + split[i - 1];
+    for (int k = 0; k < np; ++k) {
+      const int i = np - 1 - k;
+      SubGeom g;
+      g.x = static_cast<const uint4*>(k == 0 ? y : x);
+      g.y = static_cast<uint4*>(x);
+      g.tw = static_cast<const uint4*>(p->tw_inv);
+      g.n = (uint32_t)n;
+      g.s0 = (uint32_t)starts[i];
+      g.m = (uint32_t)split[i];
+      g.l = (uint32_t)(n - starts[i] - split[i]);
+      g.nsub = (uint64_t)batch << (n - split[i]);
+      if (int rc = tile_inv_pass(p, g, i == 0 ? 1 : 0, s)) return rc;
+    }
+    return BNTT_OK;
   }
   Epilogue ep;
   ep.scale = p->ninv;

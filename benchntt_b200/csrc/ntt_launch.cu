@@ -175,13 +175,13 @@ int ntt_forward_on(bntt_plan* plan, void* y, const void* x, size_t batch, cudaSt
                    const void* b, uint64_t bmask) {
   if (batch == 0) return BNTT_OK;
   const int n = (int)plan->log2n;
-  // above 2^10 points: the runtime-size engine with passes of at most 8
-  // stages (a strided pass then covers >= 8 adjacent columns, 128 B per
-  // row); measured 1.5x faster at 2^16 than compiled tiles with 10-stage
-  // passes, whose strided passes touch 2 or 4 columns per tile
+  // above 2^10 points: the persistent kernel's split on 4-element tiles
+  // (strided passes of 5..7 stages over 2^(10-m) adjacent columns, 256 B or
+  // more per row, then a contiguous pass), else the runtime-size engine with
+  // passes of at most 8 stages.  Measured at 2^16: 0.83 against 0.73 of the
+  // IMAD roofline for the engine; compiled tiles with 10-stage passes, whose
+  // strided passes touch 2 or 4 columns per row, were 1.5x slower than that.
   if (n > 10 && arith_fast(plan->ctx, plan->fast)) {
-    // the persistent kernel's split and tiles when every pass's shape is
-    // compiled, else the engine
     const std::vector<int> split = tile_split(n);
     std::vector<const SubKernel*> ks;
     int s0 = 0;
