@@ -114,7 +114,11 @@ class ClockSampler:
         import threading
         self.thread = threading.Thread(target=self._poll, daemon=True)
         self.thread.start()
-        time.sleep(0.05)
+        # the first NVML initialisation of a process can take a few hundred
+        # ms: wait for the first sample, so the timed region is covered
+        t0 = time.perf_counter()
+        while not self.samples and self.err is None and time.perf_counter() - t0 < 5.0:
+            time.sleep(0.005)
 
     def stop(self) -> dict:
         self.stop_flag = True
