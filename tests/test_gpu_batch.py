@@ -171,6 +171,42 @@ def test_run_host(ctx):
     s.close()
 
 
+def test_u128_layout_batch_forward_and_inverse(ctx):
+    """Plans in the little-endian u128 layout (the persistent kernels are
+    compiled once per layout): a mix of 2^1..2^10 plus 2^12 and 2^16 jobs,
+    forward and inverse, equal the oracle on the same values."""
+    b = W.uneven_batch(seed=33, n_small=1500, small_lo=1, small_hi=10, large=((12, 2), (16, 1)))
+    tables = {n: C.uniform_pairs(W.SEED_TWIDDLE_BASE + n, 1 << n, C.Q_NTT) for n in b.sizes}
+    plans = {n: bn.Plan(ctx, n, C.Q_NTT, C.MU_NTT, tables[n][:, ::-1].copy(), bn.LAYOUT_U128)
+             for n in b.sizes}
+    pid = {n: i for i, n in enumerate(b.sizes)}
+    eng = bn.Batch(ctx, [plans[n] for n in b.sizes])
+    x = C.uniform_pairs(W.SEED_INPUT, b.total, C.Q_NTT)
+    dx = DevBuf.from_array(ctx, x[:, ::-1].copy())
+    dy = DevBuf(ctx, b.total * 16)
+    offs = [16 * int(o) for o in b.offsets]
+    jobs = bn.Batch.jobs([dx.addr + o for o in offs], [dy.addr + o for o in offs],
+                         [pid[int(n)] for n in b.logns])
+    xs = [x[int(o):int(o) + (1 << int(n))] for o, n in zip(b.offsets, b.logns)]
+    ts = [tables[int(n)] for n in b.logns]
+    eng.run_dev(jobs)
+    assert eng.status() == bn.OK
+    want = np.concatenate(C.oracle_ntt_jobs(xs, ts, [int(n) for n in b.logns], threads=8))
+    assert np.array_equal(dy.to_array(b.total)[:, ::-1], want)
+    eng.run_inverse_dev(jobs)
+    assert eng.status() == bn.OK
+    got = dy.to_array(b.total)[:, ::-1]
+    for i in range(b.count):
+        o, n = int(b.offsets[i]), int(b.logns[i])
+        assert np.array_equal(got[o:o + (1 << n)], C.oracle_ntt_inverse(x[o:o + (1 << n)], tables[n], n)), \
+            f"job {i} (2^{n})"
+    eng.close()
+    for p in plans.values():
+        p.close()
+    dx.free()
+    dy.free()
+
+
 def test_reference_arith_batch():
     c = bn.Context(0, arith=bn.ARITH_REFERENCE)
     b = W.uneven_batch(seed=7, n_small=400, large=((12, 1),))
