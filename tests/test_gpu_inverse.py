@@ -82,8 +82,8 @@ def test_round_trip_all_sizes(ctx, logn, batch):
     p.close()
 
 
-def test_in_place_and_u128_layout(ctx):
-    logn = 10
+@pytest.mark.parametrize("logn", [10, 12])
+def test_in_place_and_u128_layout(ctx, logn):
     n = 1 << logn
     t = C.uniform_pairs(31, n, C.Q_NTT)
     y = C.uniform_pairs(32, 8 * n, C.Q_NTT)

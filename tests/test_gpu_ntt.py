@@ -120,13 +120,13 @@ def test_uniform_batch_matches_oracle(ctx, logn, batch):
     assert np.array_equal(y, C.oracle_ntt(x, t, logn, threads=8, form=1))
 
 
-@pytest.mark.parametrize("logn", [4, 10, 12])
+@pytest.mark.parametrize("logn", [4, 7, 10, 12, 16])
 def test_layout_u128(ctx, logn):
     n = 1 << logn
     x = C.uniform_pairs(61, n * 3, C.Q_NTT)
     t = C.uniform_pairs(62, n, C.Q_NTT)
     y = run_dev(ctx, hilo_to_u128(x), hilo_to_u128(t), logn, layout=bn.LAYOUT_U128)
-    assert np.array_equal(u128_to_hilo(y), C.oracle_ntt(x, t, logn))
+    assert np.array_equal(u128_to_hilo(y), C.oracle_ntt(x, t, logn, threads=8))
 
 
 @pytest.mark.parametrize("logn", [5, 10, 13])
