@@ -82,6 +82,21 @@ def test_round_trip_all_sizes(ctx, logn, batch):
     p.close()
 
 
+@pytest.mark.parametrize("logn", [15, 19, 21, 22, 23, 24])
+def test_round_trip_every_split(ctx, logn):
+    """ntt^-1(ntt(x)) = x for the sizes whose pass splits the other tests do
+    not reach: strided passes of 6 and 7 stages, contiguous last passes of
+    8 and 10 stages, up to 2^24 points (one transform)."""
+    n = 1 << logn
+    t = C.uniform_pairs(3000 + logn, n, C.Q_NTT)
+    x = C.uniform_pairs(4000 + logn, n, C.Q_NTT)
+    p = bn.Plan(ctx, logn, C.Q_NTT, C.MU_NTT, t)
+    y = forward(ctx, p, x)
+    assert not np.array_equal(y, x)
+    assert np.array_equal(inverse(ctx, p, y), x)
+    p.close()
+
+
 @pytest.mark.parametrize("logn", [10, 12])
 def test_in_place_and_u128_layout(ctx, logn):
     n = 1 << logn

@@ -111,7 +111,7 @@ def test_edge_inputs(ctx, logn, edge):
 
 @pytest.mark.parametrize("logn,batch", [(1, 7), (3, 1000), (4, 4099), (5, 333), (6, 1000),
                                         (7, 513), (8, 300), (9, 129), (10, 130), (11, 9),
-                                        (12, 5), (14, 3), (16, 2)])
+                                        (12, 5), (14, 3), (15, 2), (16, 2), (19, 1)])
 def test_uniform_batch_matches_oracle(ctx, logn, batch):
     n = 1 << logn
     x = C.uniform_pairs(7 + logn, n * batch, C.Q_NTT)
