@@ -225,7 +225,8 @@ static int make_items(const bntt_batch* b, Schedule& sc, const uint32_t per_size
       s0 += m;
     }
   }
-  sc.items.insert(sc.items.end(), sc.later[0].begin(), sc.later[0].end());
+  std::vector<WorkItem>& small = sc.small_items;
+  small.clear();
   for (int n = 10; n >= 1; --n) {
     const uint32_t cnt = per_size[n];
     if (cnt == 0) continue;
@@ -238,10 +239,25 @@ static int make_items(const bntt_batch* b, Schedule& sc, const uint32_t per_size
     for (uint32_t s = 0; s < cnt; s += tpc) {
       w.a = first[n] + s;
       w.b = std::min<uint32_t>(tpc, cnt - s);
-      sc.items.push_back(w);
+      small.push_back(w);
     }
   }
-  for (int p = 1; p < kMaxPasses; ++p) sc.items.insert(sc.items.end(), sc.later[p].begin(), sc.later[p].end());
+  // first passes, then the small tiles cut into one segment before each
+  // later pass group, so a later pass is queued well after the pass it
+  // waits for
+  int groups = 0;
+  for (int p = 1; p < kMaxPasses; ++p) groups += sc.later[p].empty() ? 0 : 1;
+  sc.items.insert(sc.items.end(), sc.later[0].begin(), sc.later[0].end());
+  size_t from = 0;
+  int seg = 0;
+  for (int p = 1; p < kMaxPasses; ++p) {
+    if (sc.later[p].empty()) continue;
+    const size_t to = small.size() * (size_t)(++seg) / (size_t)(groups + 1);
+    sc.items.insert(sc.items.end(), small.begin() + from, small.begin() + to);
+    from = to;
+    sc.items.insert(sc.items.end(), sc.later[p].begin(), sc.later[p].end());
+  }
+  sc.items.insert(sc.items.end(), small.begin() + from, small.end());
   return BNTT_OK;
 }
 

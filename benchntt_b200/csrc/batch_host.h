@@ -17,6 +17,7 @@ struct Schedule {
   std::vector<DevJob> djobs;
   std::vector<uint32_t> order;
   std::vector<WorkItem> items;
+  std::vector<WorkItem> small_items;  // make_items' scratch: the small tiles before interleaving
   std::vector<uint32_t> pass_tiles;
   std::vector<WorkItem> later[kMaxPasses];  // build scratch: pass items by run position
   std::vector<uint8_t> job_log2n;           // build scratch: each job's size
